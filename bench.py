@@ -1,0 +1,337 @@
+"""Benchmark: normal-op applies/s of the batched Toeplitz SENSE CG (4D-flow batch).
+
+Workload (default): 20 cardiac frames x 5 velocity encodings = 100 systems, 128^3
+complex64 images, 16 coils, one Toeplitz diagonal (2x grid 256^3, built in FP64 on the
+GPU from a per-frame interleaved golden-angle kooshball of 2000 spokes x 256 samples),
+15 CG iterations with lambda = 1e-3 on every system.  One step = one batched CG solve
+of all 100 systems = 100 x (1 + 15) normal-op applies.  Synthetic, seeded inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One process per GPU (torchrun for N > 1); each rank solves its own copy of the batch
+(weak scaling, no collective on the data path).  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "Normal-op applies/s (128^3, 16 coils)"
+UNIT = "applies/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--coils", type=int, default=16)
+    ap.add_argument("--frames", type=int, default=20)
+    ap.add_argument("--encodings", type=int, default=5)
+    ap.add_argument("--iters", type=int, default=15)
+    ap.add_argument("--spokes", type=int, default=2000)
+    ap.add_argument("--samples", type=int, default=256)
+    ap.add_argument("--lam", type=float, default=1e-3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(a):
+    return {
+        "workload": f"4D-flow batch: {a.frames} frames x {a.encodings} encodings, {a.n}^3 complex64, "
+                    f"{a.coils} coils, {a.iters}-iteration CG (lambda={a.lam}), per-frame kooshball "
+                    f"{a.spokes}x{a.samples}",
+        "image": [a.n] * 3, "coils": a.coils, "systems": a.frames * a.encodings, "frames": a.frames,
+        "encodings": a.encodings, "cg_iters": a.iters, "lambda": a.lam,
+        "applies_per_step": a.frames * a.encodings * (a.iters + 1),
+        "l2": "inputs larger than L2 (per-step working set ~60 GB)",
+        "parallelism": f"replicas x{a.gpus}",
+    }
+
+
+# ------------------------------------------------------------------ clocks -------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        busy = [s for s in sm if smax and s > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- CPU baseline ------
+def cpu_reference_rate(a, repeats=1, iters=2):
+    """The reference's LibTorch-CPU path (oracle/torch_ref.py) on 1 system x `iters`
+    CG iterations x all coils, with all host threads.  Returns (applies/s, sample, cores)."""
+    from hastycompute_b200 import synth
+    from oracle import torch_ref
+
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    shape = (a.n,) * 3
+    M = tuple(2 * n for n in shape)
+    rng = np.random.default_rng(0)
+    # the diagonal's values do not change the CPU path's timing; a seeded stand-in of the
+    # right shape and dtype (complex64 on the 2x grid) is used
+    T = torch.from_numpy((1.0 + 0.1 * rng.standard_normal(M)).astype(np.complex64))
+    sm = torch.from_numpy(synth.coil_maps(a.coils, shape, seed=1))
+    b = torch.from_numpy(synth.gaussian_image(shape, seed=2)).reshape((1,) + shape)
+    A = torch_ref.ToeplitzSenseNormalCPU(T, sm, lam=a.lam)
+    times = []
+    napply = 0
+    for _ in range(repeats):
+        x = torch.zeros_like(b)
+        t0 = time.perf_counter()
+        napply = torch_ref.conjugate_gradient(A, b, x, iters=iters)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    sample = (f"1 system x {iters} CG iterations ({napply} normal-op applies x {a.coils} coils) at {a.n}^3, "
+              f"median of {repeats}; applies/s extrapolates linearly to the full batch")
+    return napply / t, sample, cores
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = workload_config(a)
+    cfg["parallelism"] = "cpu"
+    for _ in range(a.warmup):
+        cpu_reference_rate(a, repeats=1, iters=1)
+    rates = []
+    sample = ""
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        r, sample, cores = cpu_reference_rate(a, repeats=1, iters=1)
+        rates.append(r)
+    wall = time.perf_counter() - t0
+    v = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1000.0 * wall / max(1, a.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm --------
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        pg = dist
+
+    from hastycompute_b200 import capi, synth
+    from hastycompute_b200.toeplitz import ToeplitzPlan
+
+    shape = (a.n,) * 3
+    nsys = a.frames * a.encodings
+    plan = ToeplitzPlan(shape, dev)
+    t_setup = time.perf_counter()
+    sm = torch.from_numpy(synth.coil_maps(a.coils, shape, seed=1)).to(dev)
+    packed = torch.empty((a.frames, plan.packed_numel()), dtype=torch.float32, device=dev)
+    for f in range(a.frames):
+        coords = torch.from_numpy(synth.kooshball(a.spokes, a.samples, frame=f, nframes=a.frames))
+        packed[f] = plan.build_diagonal(coords)
+    torch.cuda.synchronize()
+    t_diag = time.perf_counter() - t_setup
+    diag_index = [s // a.encodings for s in range(nsys)]
+    xtrue = torch.empty((nsys,) + shape, dtype=torch.complex64, device=dev)
+    for f in range(a.frames):
+        xtrue[f * a.encodings:(f + 1) * a.encodings] = torch.from_numpy(
+            synth.flow_phantom(shape, a.encodings, seed=100 + f)).to(dev)
+    b = torch.empty_like(xtrue)
+    plan.sense_normal(xtrue, b, sm, packed, diag_index=diag_index, lam=a.lam)
+    x = torch.zeros_like(b)
+    torch.cuda.synchronize()
+
+    def step():
+        x.zero_()
+        plan.cg(x, b, sm, packed, iters=a.iters, lam=a.lam, diag_index=diag_index)
+
+    for _ in range(max(3, a.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = capi.launch_count()
+    capi.profile_start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(a.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    prof = capi.profile_stop()
+    launches = capi.launch_count() - launches0
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    applies_per_step = nsys * (a.iters + 1)
+    value = world * applies_per_step * a.steps / (ms / 1000.0)
+
+    # ---- end to end through the public API with host buffers ----
+    e2e = None
+    if not a.no_e2e:
+        xh = torch.zeros((nsys,) + shape, dtype=torch.complex64).pin_memory()
+        bh = b.cpu().pin_memory()
+        outh = torch.empty_like(xh).pin_memory()
+        xd = torch.empty_like(x)
+        bd = torch.empty_like(b)
+
+        def e2e_step():
+            xd.copy_(xh, non_blocking=True)
+            bd.copy_(bh, non_blocking=True)
+            plan.cg(xd, bd, sm, packed, iters=a.iters, lam=a.lam, diag_index=diag_index)
+            outh.copy_(xd, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if pg:
+            t = torch.tensor([ems], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * applies_per_step * a.steps / (ems / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": int(xh.numel() * 8 + bh.numel() * 8), "d2h_bytes_per_step": int(outh.numel() * 8)}
+
+    # ---- roofline of the dominant kernel ----
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    U = 8.0 * a.n ** 3
+    C = a.coils
+    per_kernel = {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof.items() if v[1]}
+    # algorithmic bytes per launch of each pass (one CG normal op over all systems):
+    #  expand_fwd_x : read S_c (U) + write spill (2U) per slot, read x (U) per system
+    #  plane_yz     : read + write the spill (4U) per slot, read Re(T) (4U) per frame
+    #  inv_x_combine: read spill (2U) + S_c (U) per slot, read x (U) + write out (U) per system
+    alg = {"expand_fwd_x": (3 * C + 1) * U * nsys, "plane_yz": 4 * U * C * nsys + 4 * U * a.frames,
+           "inv_x_combine": (3 * C + 2) * U * nsys}
+    dom = max(("expand_fwd_x", "plane_yz", "inv_x_combine"), key=lambda k: prof[k][0])
+    dms = prof[dom][0] / max(1, prof[dom][1])
+    achieved = alg[dom] / (dms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_src, "traffic": None,
+                "alg_bytes_per_launch": alg[dom], "ms_per_launch": dms}
+    # whole-apply yardstick: (18C + 10) * U bytes per normal-op apply
+    b_alg = (18 * C + 10) * U
+    apply_rate_dev = applies_per_step * a.steps / (ms / 1000.0)
+    yard = {"bytes_per_apply": b_alg, "achieved_gbs": b_alg * apply_rate_dev / 1e9,
+            "frac_of_hbm": b_alg * apply_rate_dev / 1e9 / hbm}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        r, sample, cores = cpu_reference_rate(a)
+        cpu = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": max(3, a.warmup), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic (seeded)", "config": workload_config(a),
+            "cg_solves_per_s": value / (a.iters + 1), "e2e": e2e, "gpu_launches": launches,
+            "roofline": roofline, "apply_yardstick": yard, "kernels": per_kernel, "cpu_baseline": cpu,
+            "clocks": clk, "setup_s": {"diagonals": t_diag},
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,157 @@
+// Batched conjugate-gradient vector updates with FP64 reductions, kept on the device.
+//
+// Restates lib/op/opalgs.cpp:50-96 (ConjugateGradient::run) for many independent
+// systems at once.  Per iteration i (rz[i] = Re<r, r> known):
+//   normal op:   Ap = (A + lambda I) p, plus per-CTA FP64 partials of Re<p, Ap>
+//   step_xr:     pAp = sum(partials); if pAp <= 0 -> status NOT_PD (x untouched);
+//                alpha = rz[i] / pAp;  x += alpha p;  r -= alpha Ap;  partials of Re<r,r>
+//   step_p:      rz[i+1] = sum(partials); p = r + (rz[i+1] / rz[i]) p;
+//                sqrt(rz[i+1]) < tol -> status CONVERGED
+// Every CTA reduces the partial arrays itself in one fixed order, so all CTAs agree
+// bit for bit and no host synchronisation is needed.  A system whose status is not
+// RUNNING is skipped by every later kernel (active[sys] == 0).
+#pragma once
+
+#include "common.cuh"
+
+namespace hb {
+
+enum CgStatus : int { kCgRunning = 0, kCgConverged = 1, kCgNotPD = 2 };
+
+struct CgState {
+  int nsys;
+  long long nv;          // elements per system
+  float2* x;             // [nsys][nv] solution (caller)
+  const float2* b;       // [nsys][nv] right-hand side (caller)
+  float2* r;             // [nsys][nv]
+  float2* p;             // [nsys][nv]
+  float2* ap;            // [nsys][nv]
+  double* rz;            // [nsys][iters+1]
+  int rz_ld;             // iters + 1
+  int* status;           // [nsys]
+  int* active;           // [nsys]
+  int* iters_done;       // [nsys]
+  const double* pap_part;  // [nsys][npap]
+  int npap;
+  double* rr_part;       // [nsys][gridDim.x of the update kernels]
+  double tol;
+};
+
+// Deterministic block-wide sum of n doubles (same order in every CTA).
+__device__ double block_sum_fixed(const double* v, int n, double* red) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += v[i];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  __syncthreads();
+  if (lane == 0) red[warp] = s;
+  __syncthreads();
+  double tot = 0.0;
+  const int nw = blockDim.x / 32;
+  for (int w = 0; w < nw; ++w) tot += red[w];
+  __syncthreads();
+  return tot;
+}
+
+__device__ void block_write_partial(double s, double* out, double* red) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  __syncthreads();
+  if (lane == 0) red[warp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) tot += red[w];
+    *out = tot;
+  }
+}
+
+// r = b - Ap; p = r; partial Re<r, r>
+__global__ void __launch_bounds__(256) cg_init_kernel(CgState s) {
+  __shared__ double red[32];
+  const int sys = blockIdx.y;
+  const long long base = (long long)sys * s.nv;
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x) {
+    const float2 r = csub(s.b[base + i], s.ap[base + i]);
+    s.r[base + i] = r;
+    s.p[base + i] = r;
+    acc += (double)r.x * r.x + (double)r.y * r.y;
+  }
+  block_write_partial(acc, s.rr_part + (long long)sys * gridDim.x + blockIdx.x, red);
+}
+
+// rz[0] = sum of partials; status/active from tol.   grid: nsys blocks
+__global__ void __launch_bounds__(256) cg_init_finish_kernel(CgState s, int nrr) {
+  __shared__ double red[32];
+  const int sys = blockIdx.x;
+  const double rz = block_sum_fixed(s.rr_part + (long long)sys * nrr, nrr, red);
+  if (threadIdx.x == 0) {
+    s.rz[(long long)sys * s.rz_ld] = rz;
+    s.iters_done[sys] = 0;
+    const bool run = !(sqrt(rz) < s.tol);
+    s.status[sys] = run ? kCgRunning : kCgConverged;
+    s.active[sys] = run ? 1 : 0;
+  }
+}
+
+__global__ void __launch_bounds__(256) cg_step_xr_kernel(CgState s, int it) {
+  __shared__ double red[32];
+  const int sys = blockIdx.y;
+  if (!s.active[sys]) return;
+  const double pap = block_sum_fixed(s.pap_part + (long long)sys * s.npap, s.npap, red);
+  if (!(pap > 0.0)) {  // also catches NaN
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      s.status[sys] = kCgNotPD;
+      s.active[sys] = 0;
+    }
+    return;
+  }
+  const double alpha = s.rz[(long long)sys * s.rz_ld + it] / pap;
+  const float af = (float)alpha;
+  const long long base = (long long)sys * s.nv;
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x) {
+    const float2 p = s.p[base + i];
+    const float2 ap = s.ap[base + i];
+    float2 x = s.x[base + i];
+    float2 r = s.r[base + i];
+    x.x = fmaf(af, p.x, x.x);
+    x.y = fmaf(af, p.y, x.y);
+    r.x = fmaf(-af, ap.x, r.x);
+    r.y = fmaf(-af, ap.y, r.y);
+    s.x[base + i] = x;
+    s.r[base + i] = r;
+    acc += (double)r.x * r.x + (double)r.y * r.y;
+  }
+  block_write_partial(acc, s.rr_part + (long long)sys * gridDim.x + blockIdx.x, red);
+}
+
+__global__ void __launch_bounds__(256) cg_step_p_kernel(CgState s, int it) {
+  __shared__ double red[32];
+  const int sys = blockIdx.y;
+  if (!s.active[sys]) return;
+  const double rznew = block_sum_fixed(s.rr_part + (long long)sys * gridDim.x, gridDim.x, red);
+  const double rzold = s.rz[(long long)sys * s.rz_ld + it];
+  const float beta = (float)(rznew / rzold);
+  const long long base = (long long)sys * s.nv;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x) {
+    const float2 r = s.r[base + i];
+    float2 p = s.p[base + i];
+    p.x = fmaf(beta, p.x, r.x);
+    p.y = fmaf(beta, p.y, r.y);
+    s.p[base + i] = p;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s.rz[(long long)sys * s.rz_ld + it + 1] = rznew;
+    s.iters_done[sys] = it + 1;
+    if (sqrt(rznew) < s.tol) {
+      s.status[sys] = kCgConverged;
+      s.active[sys] = 0;
+    }
+  }
+}
+
+}  // namespace hb

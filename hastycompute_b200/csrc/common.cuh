@@ -1,0 +1,32 @@
+// Shared device helpers: complex float2/double2 arithmetic and status codes.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define HB_DEV __host__ __device__ __forceinline__
+
+namespace hb {
+
+HB_DEV float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+HB_DEV float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+HB_DEV float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+HB_DEV float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+HB_DEV float2 cmulc(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+HB_DEV float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+// multiply by -i (DIR = -1) or +i (DIR = +1)
+template <int DIR>
+HB_DEV float2 rot90(float2 a) {
+  return DIR < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+}
+// a * w where w is given by (c, s) = (cos, DIR*sin)
+HB_DEV float2 crot(float2 a, float c, float s) {
+  return make_float2(fmaf(a.x, c, -a.y * s), fmaf(a.x, s, a.y * c));
+}
+
+}  // namespace hb

@@ -1,0 +1,226 @@
+// Register-resident small DFTs and the "team" FFT used by every pass.
+//
+// A team of S lanes (inside one warp) transforms one line of length L = E*S; each lane
+// holds E complex values in registers.  The transform is the classic two-factor
+// (four-step) split L = E x S:
+//   forward : lane t holds x[t + S*e] (e < E)          -- layout D_in
+//             E-point DFT in registers, twiddle w_L^(t*k1), one shared-memory exchange,
+//             S-point DFTs in registers
+//             -> lane t holds X[(t + S*c) + E*k2] in v[c*S + k2]  -- layout D_out
+//   inverse : the exact transpose (D_out -> D_in), unnormalised.
+// Zero-padded inputs (upper half zero, the 2x Toeplitz embedding) and cropped outputs
+// (only the lower half needed) are pruned at compile time.
+#pragma once
+
+#include "common.cuh"
+
+namespace hb {
+
+// ---- constants: cos/sin of k*pi/8 (exact mathematical values rounded to float) ----
+constexpr float kC8 = 0.70710678118654752f;  // cos(pi/4)
+constexpr float kC16 = 0.92387953251128676f; // cos(pi/8)
+constexpr float kS16 = 0.38268343236508977f; // sin(pi/8)
+
+// multiply by exp(DIR * 2*pi*i * P / 16)
+template <int P, int DIR>
+HB_DEV float2 tw16(float2 a) {
+  constexpr int p = ((P % 16) + 16) % 16;
+  if constexpr (p == 0) return a;
+  else if constexpr (p == 4) return rot90<DIR>(a);
+  else if constexpr (p == 8) return make_float2(-a.x, -a.y);
+  else if constexpr (p == 12) return rot90<-DIR>(a);
+  else {
+    constexpr float c = (p == 1 || p == 15) ? kC16 : (p == 2 || p == 14) ? kC8 : (p == 3 || p == 13) ? kS16
+                      : (p == 5 || p == 11) ? -kS16 : (p == 6 || p == 10) ? -kC8 : -kC16;
+    constexpr float s0 = (p == 1 || p == 7) ? kS16 : (p == 2 || p == 6) ? kC8 : (p == 3 || p == 5) ? kC16
+                       : (p == 9 || p == 15) ? -kS16 : (p == 10 || p == 14) ? -kC8 : -kC16;
+    constexpr float s = DIR < 0 ? -s0 : s0;
+    return crot(a, c, s);
+  }
+}
+
+template <int DIR>
+HB_DEV void dft2(float2& a, float2& b) {
+  float2 t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+template <int DIR>
+HB_DEV void dft4(float2& v0, float2& v1, float2& v2, float2& v3) {
+  float2 t0 = cadd(v0, v2), t1 = csub(v0, v2);
+  float2 t2 = cadd(v1, v3), t3 = rot90<DIR>(csub(v1, v3));
+  v0 = cadd(t0, t2);
+  v2 = csub(t0, t2);
+  v1 = cadd(t1, t3);
+  v3 = csub(t1, t3);
+}
+
+// ---- generic natural-order DFT of size R in registers ----
+template <int R, int DIR>
+struct Dft;
+
+template <int DIR>
+struct Dft<1, DIR> {
+  static HB_DEV void run(float2*) {}
+};
+template <int DIR>
+struct Dft<2, DIR> {
+  static HB_DEV void run(float2* v) { dft2<DIR>(v[0], v[1]); }
+};
+template <int DIR>
+struct Dft<4, DIR> {
+  static HB_DEV void run(float2* v) { dft4<DIR>(v[0], v[1], v[2], v[3]); }
+};
+template <int DIR>
+struct Dft<8, DIR> {
+  static HB_DEV void run(float2* v) {
+    // radix-2 DIT over two 4-point DFTs
+    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<DIR>(e0, e1, e2, e3);
+    dft4<DIR>(o0, o1, o2, o3);
+    o1 = tw16<2, DIR>(o1);
+    o2 = tw16<4, DIR>(o2);
+    o3 = tw16<6, DIR>(o3);
+    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+  }
+};
+template <int DIR>
+struct Dft<16, DIR> {
+  // n = n1 + 4*n2, k = 4*k1 + k2: 4-point DFTs over n2, twiddle w16^(n1*k2), 4-point over n1
+  static HB_DEV void run(float2* v) {
+    float2 y[4][4];
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) {
+      y[n1][0] = v[n1]; y[n1][1] = v[n1 + 4]; y[n1][2] = v[n1 + 8]; y[n1][3] = v[n1 + 12];
+      dft4<DIR>(y[n1][0], y[n1][1], y[n1][2], y[n1][3]);
+    }
+    y[1][1] = tw16<1, DIR>(y[1][1]); y[1][2] = tw16<2, DIR>(y[1][2]); y[1][3] = tw16<3, DIR>(y[1][3]);
+    y[2][1] = tw16<2, DIR>(y[2][1]); y[2][2] = tw16<4, DIR>(y[2][2]); y[2][3] = tw16<6, DIR>(y[2][3]);
+    y[3][1] = tw16<3, DIR>(y[3][1]); y[3][2] = tw16<6, DIR>(y[3][2]); y[3][3] = tw16<9, DIR>(y[3][3]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+      float2 a = y[0][k2], b = y[1][k2], c = y[2][k2], d = y[3][k2];
+      dft4<DIR>(a, b, c, d);
+      v[k2] = a; v[4 + k2] = b; v[8 + k2] = c; v[12 + k2] = d;
+    }
+  }
+};
+
+// DFT of size R whose inputs v[R/2..R-1] are zero (they are not read).
+// X[2k] = DFT_{R/2}(v)[k];  X[2k+1] = DFT_{R/2}(v[n] * w_R^n)[k]
+template <int R, int DIR>
+struct DftHalfIn {
+  static HB_DEV void run(float2* v) {
+    constexpr int H = R / 2;
+    float2 a[H], b[H];
+#pragma unroll
+    for (int n = 0; n < H; ++n) a[n] = v[n];
+    b[0] = v[0];
+    if constexpr (R == 2) {
+    } else if constexpr (R == 4) {
+      b[1] = rot90<DIR>(v[1]);
+    } else if constexpr (R == 8) {
+      b[1] = tw16<2, DIR>(v[1]); b[2] = tw16<4, DIR>(v[2]); b[3] = tw16<6, DIR>(v[3]);
+    } else if constexpr (R == 16) {
+      b[1] = tw16<1, DIR>(v[1]); b[2] = tw16<2, DIR>(v[2]); b[3] = tw16<3, DIR>(v[3]);
+      b[4] = tw16<4, DIR>(v[4]); b[5] = tw16<5, DIR>(v[5]); b[6] = tw16<6, DIR>(v[6]);
+      b[7] = tw16<7, DIR>(v[7]);
+    } else {
+      static_assert(R <= 16, "DftHalfIn: size not supported");
+    }
+    Dft<H, DIR>::run(a);
+    Dft<H, DIR>::run(b);
+#pragma unroll
+    for (int k = 0; k < H; ++k) { v[2 * k] = a[k]; v[2 * k + 1] = b[k]; }
+  }
+};
+
+// ---- team configuration for a line of length L ----
+template <int L>
+struct TeamCfg;
+template <> struct TeamCfg<8> { static constexpr int E = 4, S = 2; };
+template <> struct TeamCfg<16> { static constexpr int E = 4, S = 4; };
+template <> struct TeamCfg<32> { static constexpr int E = 8, S = 4; };
+template <> struct TeamCfg<64> { static constexpr int E = 8, S = 8; };
+template <> struct TeamCfg<128> { static constexpr int E = 16, S = 8; };
+template <> struct TeamCfg<256> { static constexpr int E = 16, S = 16; };
+
+// Shared-memory float2 slots one team needs for its exchange buffer.  The stride is
+// chosen so that teams sharing a half-warp land on disjoint banks.
+template <int L>
+constexpr int team_buf_stride() {
+  constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+  constexpr int base = E * (S + 1);
+  constexpr int want = S % 16;
+  return base + ((want - base % 16) + 32) % 16;
+}
+
+// Forward (DIR=-1) or inverse (DIR=+1) transform D_in -> D_out.
+//   v    : E registers, v[e] = x[t + S*e]; on return v[c*S + k2] = X[(t+S*c) + E*k2]
+//   tw   : table of L entries, tw[k1*S + t] = exp(-2*pi*i*t*k1/L)  (forward sign)
+//   buf  : this team's exchange buffer (team_buf_stride<L>() float2)
+template <int L, int DIR, bool HALF_IN>
+__device__ __forceinline__ void team_fft_din_to_dout(float2* v, int t, float2* buf, const float2* tw) {
+  constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+  if constexpr (HALF_IN) DftHalfIn<E, DIR>::run(v);
+  else Dft<E, DIR>::run(v);
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) {
+    float2 w = tw[k1 * S + t];
+    if (DIR > 0) w.y = -w.y;
+    buf[k1 * (S + 1) + t] = cmul(v[k1], w);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < E / S; ++c) {
+    float2 u[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) u[j] = buf[(t + S * c) * (S + 1) + j];
+    Dft<S, DIR>::run(u);
+#pragma unroll
+    for (int k2 = 0; k2 < S; ++k2) v[c * S + k2] = u[k2];
+  }
+  __syncwarp();
+}
+
+// Transpose of the above: D_out -> D_in.  With HALF_OUT only v[0..E/2) (x[n], n < L/2)
+// are meaningful on return.
+template <int L, int DIR, bool HALF_OUT>
+__device__ __forceinline__ void team_fft_dout_to_din(float2* v, int t, float2* buf, const float2* tw) {
+  constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+#pragma unroll
+  for (int c = 0; c < E / S; ++c) {
+    float2 u[S];
+#pragma unroll
+    for (int k2 = 0; k2 < S; ++k2) u[k2] = v[c * S + k2];
+    Dft<S, DIR>::run(u);
+#pragma unroll
+    for (int j = 0; j < S; ++j) buf[(t + S * c) * (S + 1) + j] = u[j];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) {
+    float2 w = tw[k1 * S + t];
+    if (DIR > 0) w.y = -w.y;
+    v[k1] = cmul(buf[k1 * (S + 1) + t], w);
+  }
+  __syncwarp();
+  Dft<E, DIR>::run(v);
+  (void)HALF_OUT;  // unused outputs are removed by dead-code elimination
+}
+
+// Index helpers for the two layouts.
+template <int L>
+HB_DEV int din_index(int t, int e) { return t + TeamCfg<L>::S * e; }
+template <int L>
+HB_DEV int dout_index(int t, int r) {  // r = c*S + k2
+  constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+  return (t + S * (r / S)) + E * (r % S);
+}
+
+}  // namespace hb

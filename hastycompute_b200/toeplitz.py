@@ -1,0 +1,220 @@
+"""Python host layer over the C ABI, on torch device tensors.
+
+Mirrors the reference operator semantics:
+
+* ``ToeplitzPlan.build_diagonal`` / ``pack_diagonal`` -- ``CUDANormalNufftToeplitz``'s
+  diagonal construction (``lib/fft/nufft.cpp:932-1053``) and the from-diagonal
+  constructor (``nufft.cpp:1133-1161``).
+* ``ToeplitzPlan.apply`` / ``apply_add`` / ``apply_addcmul`` / ``apply_inplace`` --
+  ``nufft.cpp:1163-1197`` (``apply`` returns a view into ``storage2`` as the reference
+  does).
+* ``ToeplitzPlan.sense_normal`` -- ``sense_normal_apply`` with the Toeplitz body
+  (``lib/mri/sense.ixx:500-578``), batched over systems and frames.
+* ``ToeplitzPlan.cg`` -- ``ConjugateGradient::run`` (``lib/op/opalgs.cpp:50-96``) on
+  ``A + lambda*I`` for many systems at once.
+
+Every call goes to ``libhasty_b200.so``; there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import capi
+
+
+def _stream_ptr(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _check_c64(t, name, device, shape=None):
+    if t.dtype != torch.complex64:
+        raise RuntimeError(f"{name} must be complex64")
+    if t.device != device:
+        raise RuntimeError(f"{name} must reside on {device}")
+    if not t.is_contiguous():
+        raise RuntimeError(f"{name} must be contiguous")
+    if shape is not None and tuple(t.shape[-len(shape):]) != tuple(shape):
+        raise RuntimeError(f"{name} has shape {tuple(t.shape)}, expected (..., {shape})")
+
+
+class ToeplitzPlan:
+    """Geometry of an nz x ny x nx image and its 2x Toeplitz grid on one CUDA device."""
+
+    def __init__(self, nmodes, device=None):
+        self.lib = capi.load()
+        if len(nmodes) == 4:  # reference convention [ntransf, nz, ny, nx]
+            if nmodes[0] != 1:
+                raise RuntimeError("only ntransf = 1 is supported")
+            nmodes = nmodes[1:]
+        self.shape = tuple(int(n) for n in nmodes)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        if self.device.type != "cuda":
+            raise RuntimeError("ToeplitzPlan needs a CUDA device")
+        idx = self.device.index if self.device.index is not None else torch.cuda.current_device()
+        self.device = torch.device("cuda", idx)
+        h = ctypes.c_void_p()
+        capi.check(self.lib.hb_plan_create(ctypes.byref(h), *self.shape, idx))
+        self._h = h
+        self._ws = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self.lib.hb_plan_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def grid(self):
+        return tuple(2 * n for n in self.shape)
+
+    def packed_numel(self):
+        return int(self.lib.hb_diag_packed_floats(self._h))
+
+    def _workspace(self, nbytes):
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    # ---------------------------------------------------------------- diagonal ----
+    def build_diagonal(self, coords, want_complex=False):
+        """FP64 construction of T from a trajectory coords [3, K] float32 (radians).
+
+        Returns the packed diagonal (float32) and, if requested, the reference-layout
+        complex64 T [2nz, 2ny, 2nx]."""
+        if coords.dtype != torch.float32 or coords.dim() != 2 or coords.shape[0] != 3:
+            raise RuntimeError("coords must be float32 [3, K]")
+        coords = coords.to(self.device).contiguous()
+        K = coords.shape[1]
+        packed = torch.empty(self.packed_numel(), dtype=torch.float32, device=self.device)
+        T = torch.empty(self.grid, dtype=torch.complex64, device=self.device) if want_complex else None
+        nb = self.lib.hb_diag_build_workspace_bytes(self._h, K)
+        ws = torch.empty(int(nb), dtype=torch.uint8, device=self.device)
+        capi.check(self.lib.hb_diag_build(self._h, _ptr(coords), K, _ptr(packed), _ptr(T), _ptr(ws), nb,
+                                          _stream_ptr(self.device)))
+        return (packed, T) if want_complex else packed
+
+    def pack_diagonal(self, T):
+        """Pack a reference-layout diagonal [(1,) 2nz, 2ny, 2nx] complex64."""
+        T = T.reshape(self.grid)
+        _check_c64(T, "diagonal", self.device, self.grid)
+        packed = torch.empty(self.packed_numel(), dtype=torch.float32, device=self.device)
+        capi.check(self.lib.hb_diag_pack(self._h, _ptr(T), _ptr(packed), _stream_ptr(self.device)))
+        return packed
+
+    # ------------------------------------------------------- Toeplitz normal op ----
+    def _toeplitz(self, x, out, ldz, ldy, mul, accumulate, packed):
+        _check_c64(x, "in", self.device, self.shape)
+        if mul is not None:
+            _check_c64(mul, "mul", self.device, self.shape)
+        nb = self.lib.hb_normal_workspace_bytes(self._h, 1, 1)
+        ws = self._workspace(nb)
+        capi.check(self.lib.hb_toeplitz_apply(self._h, _ptr(x), _ptr(out), ldz, ldy, _ptr(mul), int(accumulate),
+                                              _ptr(packed), _ptr(ws), nb, _stream_ptr(self.device)))
+
+    def apply(self, x, packed, storage2=None):
+        """``apply`` (nufft.cpp:1163-1170): the result is written into storage2 (2x grid)
+        and the cropped view [:nz, :ny, :nx] of it is returned."""
+        if storage2 is None:
+            storage2 = torch.empty((1,) + self.grid, dtype=torch.complex64, device=self.device)
+        s2 = storage2.reshape(self.grid)
+        _check_c64(s2, "storage2", self.device, self.grid)
+        M0, M1, M2 = self.grid
+        self._toeplitz(x, s2, M1 * M2, M2, None, 0, packed)
+        view = storage2[..., : self.shape[0], : self.shape[1], : self.shape[2]]
+        return view
+
+    def apply_add(self, x, add_to, packed):
+        _check_c64(add_to, "add_to", self.device, self.shape)
+        n0, n1, n2 = self.shape
+        self._toeplitz(x, add_to, n1 * n2, n2, None, 1, packed)
+
+    def apply_addcmul(self, x, add_to, mul, packed):
+        _check_c64(add_to, "add_to", self.device, self.shape)
+        n0, n1, n2 = self.shape
+        self._toeplitz(x, add_to, n1 * n2, n2, mul, 1, packed)
+
+    def apply_inplace(self, x, packed):
+        n0, n1, n2 = self.shape
+        self._toeplitz(x, x, n1 * n2, n2, None, 0, packed)
+
+    # ------------------------------------------------------------ SENSE normal ----
+    def sense_normal(self, x, out, smaps, packed, coils=None, diag_index=None, lam=0.0, workspace_bytes=None):
+        """out[s] = sum_c conj(S_c) Top_{d(s)}(S_c x[s]) + lam x[s] for every system s.
+
+        x, out: [nsys, nz, ny, nx] (or [nz, ny, nx]); smaps [C, nz, ny, nx];
+        packed: one packed diagonal or [ndiag, packed]; diag_index: per system."""
+        x4 = x.reshape((-1,) + self.shape)
+        out4 = out.reshape((-1,) + self.shape)
+        _check_c64(x4, "in", self.device, self.shape)
+        _check_c64(out4, "out", self.device, self.shape)
+        _check_c64(smaps, "smaps", self.device, self.shape)
+        nsys = x4.shape[0]
+        if coils is None:
+            coils = list(range(smaps.shape[0]))
+        if any(c < 0 or c >= smaps.shape[0] for c in coils):
+            raise RuntimeError("coil index out of range")
+        self._check_packed(packed, diag_index, nsys)
+        ca = capi.i64_array(coils)
+        da = capi.i64_array(diag_index) if diag_index is not None else None
+        nb = self.lib.hb_normal_workspace_bytes(self._h, nsys, len(coils))
+        if workspace_bytes is not None:
+            nb = min(nb, int(workspace_bytes))
+        ws = self._workspace(nb)
+        capi.check(self.lib.hb_sense_normal_apply(self._h, nsys, _ptr(x4), _ptr(out4), _ptr(smaps), ca, len(coils),
+                                                  _ptr(packed), da, float(lam), _ptr(ws), nb,
+                                                  _stream_ptr(self.device)))
+        return out
+
+    def _check_packed(self, packed, diag_index, nsys):
+        if packed.dtype != torch.float32 or not packed.is_contiguous() or packed.device != self.device:
+            raise RuntimeError("packed diagonal must be a contiguous float32 tensor on the plan's device")
+        nd = packed.numel() // self.packed_numel()
+        if nd * self.packed_numel() != packed.numel() or nd < 1:
+            raise RuntimeError("packed diagonal has the wrong size")
+        if diag_index is not None:
+            if len(diag_index) != nsys:
+                raise RuntimeError("diag_index must have one entry per system")
+            if any(d < 0 or d >= nd for d in diag_index):
+                raise RuntimeError("diag_index out of range")
+
+    # ---------------------------------------------------------------------- CG ----
+    def cg(self, x, b, smaps, packed, iters=30, tol=0.0, lam=0.0, coils=None, diag_index=None,
+           workspace_bytes=None, raise_not_pd=True):
+        """Batched CG (opalgs.cpp:50-96) on (A^H A)_toep + lam I; x is updated in place.
+
+        Returns (status, iters_done) as lists (one per system)."""
+        x4 = x.reshape((-1,) + self.shape)
+        b4 = b.reshape((-1,) + self.shape)
+        _check_c64(x4, "x", self.device, self.shape)
+        _check_c64(b4, "b", self.device, self.shape)
+        _check_c64(smaps, "smaps", self.device, self.shape)
+        nsys = x4.shape[0]
+        if b4.shape[0] != nsys:
+            raise RuntimeError("x and b must hold the same number of systems")
+        if coils is None:
+            coils = list(range(smaps.shape[0]))
+        self._check_packed(packed, diag_index, nsys)
+        ca = capi.i64_array(coils)
+        da = capi.i64_array(diag_index) if diag_index is not None else None
+        nb = self.lib.hb_cg_workspace_bytes(self._h, nsys, len(coils), int(iters))
+        if workspace_bytes is not None:
+            nb = min(nb, int(workspace_bytes))
+        ws = self._workspace(max(nb, 1))
+        status = (ctypes.c_int32 * nsys)()
+        done = (ctypes.c_int32 * nsys)()
+        code = self.lib.hb_cg_run(self._h, nsys, _ptr(x4), _ptr(b4), _ptr(smaps), ca, len(coils), _ptr(packed), da,
+                                  float(lam), int(iters), float(tol), status, done, _ptr(ws), nb,
+                                  _stream_ptr(self.device))
+        if code == capi.HB_ERR_NOT_PD and not raise_not_pd:
+            return list(status), list(done)
+        capi.check(code)
+        return list(status), list(done)

@@ -1,0 +1,149 @@
+/*
+ * hasty_b200.h -- C ABI of the B200 (sm_100a) Toeplitz-embedded SENSE normal operator
+ * and its batched conjugate-gradient solver.
+ *
+ * Plain pointers and sizes only.  Complex arrays are interleaved complex64
+ * (float re, float im), C-contiguous, in the reference's axis order: an image is
+ * [nz][ny][nx] (x fastest), the 2x Toeplitz grid is [2nz][2ny][2nx].  All data pointers
+ * are DEVICE pointers on the plan's device unless a parameter says "host".
+ * `stream` is a cudaStream_t (NULL = legacy default stream).  Every call is
+ * asynchronous on `stream` unless documented otherwise.
+ *
+ * Every function returns HB_OK (0) or an error code; hb_last_error() gives the
+ * message of the last failure on the calling thread.  No function aborts the process
+ * or traps on the device.
+ *
+ * Reference interfaces replaced (HastyCompute, paths inside that project):
+ *   hb_diag_build / hb_diag_pack   hasty::fft::CUDANormalNufftToeplitz::build_diagonal
+ *                                  (lib/fft/nufft.cpp:932-1053, decl nufft.ixx:234-259)
+ *                                  and the from-diagonal constructor (nufft.cpp:1133-1161)
+ *   hb_toeplitz_apply              CUDANormalNufftToeplitz::apply / apply_add /
+ *                                  apply_addcmul / apply_inplace (nufft.cpp:1163-1197)
+ *   hb_sense_normal_apply          hasty::mri::sense_normal_apply with the Toeplitz body
+ *                                  (lib/mri/sense.ixx:500-578; CUDASenseNormal::apply
+ *                                  sense.ixx:274-282) and BatchedSenseNormal::apply over
+ *                                  outer batches (lib/mri/batch_sense.cpp:349-450)
+ *   hb_cg_run                      hasty::op::ConjugateGradient::run (lib/op/opalgs.cpp:50-96)
+ *                                  and BatchedConjugateGradient::run (opalgs.ixx:93-121)
+ */
+#ifndef HASTY_B200_H
+#define HASTY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HB_OK 0
+#define HB_ERR_INVALID 1     /* bad argument (null pointer, size, alignment)       */
+#define HB_ERR_UNSUPPORTED 2 /* image size not compiled in                          */
+#define HB_ERR_CUDA 3        /* CUDA runtime error                                  */
+#define HB_ERR_WORKSPACE 4   /* workspace smaller than required                     */
+#define HB_ERR_NOT_PD 5      /* CG: p^H A p <= 0 ("A was not positive definite")    */
+
+/* CG per-system status codes (hb_cg_run status_host) */
+#define HB_CG_RUNNING 0
+#define HB_CG_CONVERGED 1
+#define HB_CG_NOT_PD 2
+
+typedef struct hb_plan hb_plan;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int hb_version(void);
+
+/* Message of the last error on this thread ("" if none). */
+const char* hb_last_error(void);
+
+/* True (1) if an image of nz x ny x nx is supported by the compiled kernels. */
+int hb_size_supported(int64_t nz, int64_t ny, int64_t nx);
+
+/* Geometry plan for images nz x ny x nx on `device`: uploads the twiddle tables
+ * (allocates a few KB of device memory).  Replaces the geometry part of the
+ * CUDANormalNufftToeplitz constructors (nufft.cpp:1055-1161). */
+int hb_plan_create(hb_plan** plan, int64_t nz, int64_t ny, int64_t nx, int device);
+int hb_plan_destroy(hb_plan* plan);
+
+/* Number of floats of one packed diagonal (= 8 * nz * ny * nx). */
+int64_t hb_diag_packed_floats(const hb_plan* plan);
+
+/* Pack a reference-layout diagonal T [2nz][2ny][2nx] complex64 into the internal
+ * layout the normal operator reads (real part only; the imaginary part of T only acts
+ * on the cropped-away Nyquist offsets).  Replaces taking ownership of `diagonal` in
+ * CUDANormalNufftToeplitz(at::Tensor&& diagonal, nmodes) (nufft.cpp:1133-1161). */
+int hb_diag_pack(const hb_plan* plan, const void* T_complex, float* packed, void* stream);
+
+/* Workspace bytes for hb_diag_build with `nsamples` sample points. */
+size_t hb_diag_build_workspace_bytes(const hb_plan* plan, int64_t nsamples);
+
+/* Build the Toeplitz diagonal of a trajectory (build_diagonal, nufft.cpp:932-1053):
+ * coords: float [3][nsamples] device (row a pairs with image axis a: z, y, x; radians
+ * in [-pi, pi)).  Writes the packed diagonal (if `packed` != NULL) and/or the
+ * reference-layout complex64 T [2nz][2ny][2nx] (if `T_complex` != NULL).  FP64
+ * arithmetic throughout. */
+int hb_diag_build(const hb_plan* plan, const float* coords, int64_t nsamples, float* packed,
+                  void* T_complex, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Workspace bytes of hb_sense_normal_apply for nsys systems of ncoil coils (all in one
+ * launch); hb_toeplitz_apply needs hb_normal_workspace_bytes(plan, 1, 1). */
+size_t hb_normal_workspace_bytes(const hb_plan* plan, int64_t nsys, int64_t ncoil);
+
+/* Single Toeplitz normal op (no coils), nufft.cpp:1163-1197:
+ *   y = crop(IFFT(T * FFT(pad(in))))
+ *   out[z*out_ldz + y*out_ldy + x] (=|+=) y * (mul ? mul : 1)
+ * accumulate = 0: apply / apply_inplace (out may alias in); 1: apply_add / apply_addcmul. */
+int hb_toeplitz_apply(const hb_plan* plan, const void* in, void* out, int64_t out_ldz,
+                      int64_t out_ldy, const void* mul, int accumulate, const float* packed_diag,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* Toeplitz SENSE normal op over nsys independent systems:
+ *   out[s] = sum_{c in coils} conj(S_c) * Top_{d(s)}(S_c * x[s]) + lambda * x[s]
+ * x, out: [nsys][nz][ny][nx]; smaps: [ncoil_total][nz][ny][nx];
+ * coils: host array [ncoil] of indices into smaps; packed_diags: [ndiag][packed];
+ * diag_index: host array [nsys] (NULL = diagonal 0 for every system).
+ * out must not alias x.  Systems are processed in groups that fit the workspace. */
+int hb_sense_normal_apply(const hb_plan* plan, int64_t nsys, const void* x, void* out,
+                          const void* smaps, const int64_t* coils, int64_t ncoil,
+                          const float* packed_diags, const int64_t* diag_index, float lambda,
+                          void* workspace, size_t workspace_bytes, void* stream);
+
+/* Workspace bytes of hb_cg_run for nsys systems handled at once. */
+size_t hb_cg_workspace_bytes(const hb_plan* plan, int64_t nsys, int64_t ncoil, int iters);
+
+/* Batched CG on (A^H A)_toeplitz + lambda I, opalgs.cpp:50-96 per system:
+ * x: [nsys][image] initial guess, overwritten with the solution; b: right-hand sides.
+ * Runs `iters` iterations (stops a system early when sqrt(r^H r) < tol).
+ * status_host / iters_done_host: optional host arrays [nsys], filled on return.
+ * This call synchronises `stream` before it returns (the reference reads the CG
+ * scalars on the host too).  Returns HB_ERR_NOT_PD if any system hit p^H A p <= 0
+ * (that system's x is left at its last valid iterate). */
+int hb_cg_run(const hb_plan* plan, int64_t nsys, void* x, const void* b, const void* smaps,
+              const int64_t* coils, int64_t ncoil, const float* packed_diags,
+              const int64_t* diag_index, float lambda, int iters, double tol,
+              int32_t* status_host, int32_t* iters_done_host, void* workspace,
+              size_t workspace_bytes, void* stream);
+
+/* ---- measurement hooks (no counterpart in the reference; used by benchmarks) ----
+ * Kernel kinds for the profile counters. */
+#define HB_KERNEL_EXPAND_FWD_X 0   /* pass A */
+#define HB_KERNEL_PLANE_YZ 1       /* pass B */
+#define HB_KERNEL_INV_X_COMBINE 2  /* pass C */
+#define HB_KERNEL_CG_UPDATE 3      /* CG vector updates / reductions */
+#define HB_KERNEL_DIAG 4           /* diagonal construction / packing */
+#define HB_KERNEL_KINDS 5
+
+/* Total number of kernels this library has launched in this process. */
+uint64_t hb_launch_count(void);
+
+/* Start recording a CUDA event pair around every kernel launch (on the launching
+ * stream).  hb_profile_stop synchronises the recorded events, writes per-kind total
+ * device milliseconds and launch counts (arrays of `nkinds`), and stops recording. */
+int hb_profile_start(void);
+int hb_profile_stop(double* ms, int64_t* launches, int nkinds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HASTY_B200_H */

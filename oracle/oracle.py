@@ -1,0 +1,174 @@
+"""FP64 CPU oracle for the Toeplitz-embedded SENSE normal operator and its CG solver.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import it.
+The product path (``hastycompute_b200``) never calls it.
+
+It restates, in numpy float64, the reference algorithm (HastyCompute, C++ over
+LibTorch).  File references below are paths inside the reference project:
+
+* ``lib/fft/nufft.cpp:932-971``   ``build_diagonal_base``: a unit impulse at index
+  M/2 of the 2x grid, NUFFT type-2 (isign -1) then type-1 (isign +1), each scaled
+  by ``1/sqrt(prod(M))`` (``nufft.cpp:104-123``), then ``ifftshift`` and ``fftn``.
+  A type-2 NUFFT of a centred impulse is a constant, so the construction equals the
+  direct NUDFT  ``psf(d) = prod(M)^-1 * sum_j exp(+i c_j . d)``  for d in [-N, N)^3,
+  stored circulantly (index n <-> d = n for n < M/2, d = n - M otherwise).
+  Here it is evaluated exactly (float64, no NUFFT tolerance).
+* ``lib/fft/nufft.cpp:1163-1197``  ``apply``/``apply_add``/``apply_addcmul``/
+  ``apply_inplace``: ``y = ifftn(T * fftn(x, s=M))[:N0, :N1, :N2]`` (high-end zero
+  pad, inverse scaled by 1/prod(M)).
+* ``lib/mri/sense.ixx:500-578``  ``sense_normal_apply`` with the Toeplitz body
+  (``apply_addcmul(x*S_c, out, conj(S_c))``): ``out = sum_c conj(S_c) * Top(S_c * x)``.
+* ``lib/op/opalgs.cpp:50-96``  ``ConjugateGradient::run`` (r = b - A x, p = z, the
+  tol test on sqrt(rz), the positive-definiteness check) applied to ``A + lambda*I``
+  (``python/python/hastypy/base/torch_opalg.py:49-61``).
+* ``lib/fft/nufft.cpp:410-767`` / ``:785-920`` explicit NUFFT normal op on the N grid
+  (type-2 then type-1, each /sqrt(prod(N))), evaluated as a dense direct NUDFT.
+  ``Toeplitz = explicit / 2^3`` in 3D because of the two different grid scalings.
+
+Coordinate convention (``nufft.cpp:192-197``, ``:578-585``): ``coords`` is [3, K];
+row a pairs with image axis a (z, y, x order, x fastest in memory).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def grid2(nmodes):
+    """The Toeplitz embedding grid: every spatial axis doubled (``nufft.cpp:978-981``)."""
+    return tuple(2 * int(n) for n in nmodes)
+
+
+def _axis_phasors(c, d):
+    """exp(+i * c_j * d) for a coordinate row c [K] and integer offsets d [L] -> [K, L]."""
+    return np.exp(1j * np.outer(np.asarray(c, np.float64), np.asarray(d, np.float64)))
+
+
+def _circ_offsets(m):
+    """Signed offset d for every index n of a length-m circulant axis."""
+    n = np.arange(m)
+    return np.where(n < m // 2, n, n - m)
+
+
+def psf_circulant(coords, nmodes, weights=None, chunk=4096):
+    """PSF on the 2x grid in circulant layout (``nufft.cpp:932-971`` after ifftshift).
+
+    psf[n0,n1,n2] = prod(M)^-1 * sum_j w_j exp(+i (c0_j d0 + c1_j d1 + c2_j d2)).
+    """
+    coords = np.asarray(coords, np.float64)
+    M = grid2(nmodes)
+    K = coords.shape[1]
+    w = np.ones(K) if weights is None else np.asarray(weights, np.float64)
+    out = np.zeros(M, np.complex128)
+    d = [_circ_offsets(m) for m in M]
+    for s in range(0, K, chunk):
+        e = slice(s, min(K, s + chunk))
+        pz = _axis_phasors(coords[0, e], d[0]) * w[e, None]
+        py = _axis_phasors(coords[1, e], d[1])
+        px = _axis_phasors(coords[2, e], d[2])
+        pzy = (pz[:, :, None] * py[:, None, :]).reshape(pz.shape[0], -1)
+        out += (pzy.T @ px).reshape(M)
+    return out / float(np.prod(M))
+
+
+def toeplitz_diagonal(coords, nmodes, weights=None):
+    """T = fftn(psf) on the 2x grid, complex128 [M0, M1, M2] (``nufft.cpp:967-969``)."""
+    return np.fft.fftn(psf_circulant(coords, nmodes, weights))
+
+
+def toeplitz_apply(x, T):
+    """``CUDANormalNufftToeplitz::apply`` (``nufft.cpp:1163-1170``): crop(ifftn(T*fftn(pad x)))."""
+    x = np.asarray(x, np.complex128)
+    N = x.shape
+    F = np.fft.fftn(x, s=T.shape, axes=(0, 1, 2))
+    y = np.fft.ifftn(F * T)
+    return y[: N[0], : N[1], : N[2]]
+
+
+def sense_normal_toeplitz(x, smaps, T, coils=None):
+    """Toeplitz SENSE normal op (``sense.ixx:500-578`` + ``nufft.cpp:1181-1188``).
+
+    out.zero_(); for c in coils: out += conj(S_c) * Top(S_c * x)
+    """
+    x = np.asarray(x, np.complex128)
+    smaps = np.asarray(smaps, np.complex128)
+    if coils is None:
+        coils = range(smaps.shape[0])
+    out = np.zeros_like(x)
+    for c in coils:
+        out += np.conj(smaps[c]) * toeplitz_apply(x * smaps[c], T)
+    return out
+
+
+def explicit_normal(x, coords, weights=None):
+    """Explicit NUFFT normal op on the N grid (type-2 isign -1, type-1 isign +1, each
+    scaled 1/sqrt(prod(N)); ``nufft.cpp:104-123,785-920``), as a dense direct NUDFT."""
+    x = np.asarray(x, np.complex128)
+    coords = np.asarray(coords, np.float64)
+    N = x.shape
+    K = coords.shape[1]
+    w = np.ones(K) if weights is None else np.asarray(weights, np.float64)
+    k = [np.arange(n) - n // 2 for n in N]  # CMCL mode ordering
+    ez = _axis_phasors(coords[0], k[0])
+    ey = _axis_phasors(coords[1], k[1])
+    ex = _axis_phasors(coords[2], k[2])
+    # type 2: f_j = sum_k x_k exp(-i k.c_j)
+    f = np.einsum("jz,jy,jx,zyx->j", ez.conj(), ey.conj(), ex.conj(), x, optimize=True)
+    f = f * w
+    # type 1: y_k = sum_j f_j exp(+i k.c_j)
+    y = np.einsum("j,jz,jy,jx->zyx", f, ez, ey, ex, optimize=True)
+    return y / float(np.prod(N))
+
+
+def vdot(a, b):
+    """``vdot`` (``lib/op/vec.cpp:624-637``): sum(conj(a) * b)."""
+    return np.vdot(np.asarray(a).ravel(), np.asarray(b).ravel())
+
+
+class NotPositiveDefinite(RuntimeError):
+    pass
+
+
+def conjugate_gradient(A, b, x0=None, iters=30, tol=0.0, P=None):
+    """``ConjugateGradient::run`` (``lib/op/opalgs.cpp:50-96``), float64.
+
+    Returns (x, n_done) where n_done counts the iterations that updated x.
+    """
+    b = np.asarray(b, np.complex128)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.complex128)
+    if iters < 1:
+        return x, 0
+    r = b - A(x)
+    z = P(r) if P is not None else r
+    p = z.copy()
+    rzold = vdot(r, z).real
+    resid = np.sqrt(rzold)
+    done = 0
+    for _ in range(iters):
+        if resid < tol:
+            return x, done
+        Ap = A(p)
+        pAp = vdot(p, Ap).real
+        if pAp <= 0.0:
+            raise NotPositiveDefinite("A was not positive definite")
+        alpha = rzold / pAp
+        x = x + alpha * p
+        r = r - alpha * Ap
+        z = P(r) if P is not None else r
+        rznew = vdot(r, z).real
+        p = p * (rznew / rzold) + z
+        rzold = rznew
+        resid = np.sqrt(rzold)
+        done += 1
+    return x, done
+
+
+def regularized(A, lam):
+    """``A + lambda*I`` (``hastypy/base/torch_opalg.py:49-61``)."""
+    return lambda v: A(v) + lam * v
+
+
+def rel_l2(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))

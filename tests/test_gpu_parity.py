@@ -1,0 +1,224 @@
+"""GPU parity of the sm_100a path (through the C ABI) against the FP64 oracle.
+
+Tolerance: relative L2 <= 1e-5 for the FP32 path (FP32 FFT arithmetic vs FP64)."""
+import numpy as np
+import pytest
+import torch
+
+from hastycompute_b200 import capi, synth
+from hastycompute_b200.toeplitz import ToeplitzPlan
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _c64(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a).astype(np.complex64)).to(dev)
+
+
+def _np(t):
+    return t.detach().cpu().numpy().astype(np.complex128)
+
+
+def _case(shape, ncoil, K, seed):
+    rng = np.random.default_rng(seed)
+    coords = rng.uniform(-np.pi, np.pi, (3, K)).astype(np.float32)
+    x = synth.gaussian_image(shape, seed=seed + 1)
+    sm = synth.coil_maps(ncoil, shape, seed=seed + 2)
+    T = O.toeplitz_diagonal(coords.astype(np.float64), shape)
+    return coords, x, sm, T
+
+
+SHAPES = [(8, 8, 8), (8, 16, 32), (32, 8, 16), (16, 16, 16), (32, 32, 32), (64, 32, 16)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_toeplitz_apply_modes(cuda, shape):
+    coords, x, sm, T = _case(shape, 1, 300, 11)
+    plan = ToeplitzPlan(shape, cuda)
+    packed = plan.pack_diagonal(_c64(T, cuda))
+    xt = _c64(x, cuda)
+    ref = O.toeplitz_apply(x, T)
+    # apply: view into storage2
+    s2 = torch.zeros((1,) + plan.grid, dtype=torch.complex64, device=cuda)
+    y = plan.apply(xt, packed, s2)
+    assert O.rel_l2(_np(y[0]), ref) < TOL
+    # apply_add
+    add_to = _c64(sm[0], cuda)
+    plan.apply_add(xt, add_to, packed)
+    assert O.rel_l2(_np(add_to), sm[0] + ref) < TOL
+    # apply_addcmul
+    mul = np.conj(sm[0])
+    add_to = _c64(sm[0], cuda)
+    plan.apply_addcmul(xt, add_to, _c64(mul, cuda), packed)
+    assert O.rel_l2(_np(add_to), sm[0] + ref * mul) < TOL
+    # apply_inplace
+    xi = xt.clone()
+    plan.apply_inplace(xi, packed)
+    assert O.rel_l2(_np(xi), ref) < TOL
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (16, 8, 32), (16, 16, 16)])
+def test_diagonal_build_fp64(cuda, shape):
+    coords, x, sm, T = _case(shape, 1, 1000, 12)
+    plan = ToeplitzPlan(shape, cuda)
+    packed, Tg = plan.build_diagonal(torch.from_numpy(coords), want_complex=True)
+    assert O.rel_l2(_np(Tg), T) < 1e-6
+    packed_ref = plan.pack_diagonal(_c64(T, cuda))
+    assert O.rel_l2(packed.cpu().numpy(), packed_ref.cpu().numpy()) < 1e-6
+
+
+def test_diagonal_build_on_grid_samples(cuda):
+    """Samples exactly on grid frequencies (the Dirichlet kernel's removable singularity)."""
+    shape = (8, 8, 8)
+    c = np.zeros((3, 64), np.float32)
+    c[:, 1:] = (np.random.default_rng(3).integers(-8, 8, (3, 63)) * (2 * np.pi / 16)).astype(np.float32)
+    T = O.toeplitz_diagonal(c.astype(np.float64), shape)
+    plan = ToeplitzPlan(shape, cuda)
+    _, Tg = plan.build_diagonal(torch.from_numpy(c), want_complex=True)
+    assert O.rel_l2(_np(Tg), T) < 1e-6
+
+
+@pytest.mark.parametrize("shape,ncoil", [((16, 16, 16), 4), ((8, 16, 32), 3), ((32, 32, 32), 8)])
+def test_sense_normal_batched(cuda, shape, ncoil):
+    rng = np.random.default_rng(13)
+    plan = ToeplitzPlan(shape, cuda)
+    sm = synth.coil_maps(ncoil, shape, seed=5)
+    Ts = [O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 400)), shape) for _ in range(2)]
+    packed = torch.cat([plan.pack_diagonal(_c64(T, cuda)) for T in Ts])
+    nsys = 3
+    xs = np.stack([synth.gaussian_image(shape, seed=20 + s) for s in range(nsys)])
+    diag_index = [1, 0, 1]
+    coils = [ncoil - 1] + list(range(ncoil - 1))[::2]  # a permuted subset
+    lam = 1e-3
+    out = torch.empty((nsys,) + shape, dtype=torch.complex64, device=cuda)
+    plan.sense_normal(_c64(xs, cuda), out, _c64(sm, cuda), packed, coils=coils, diag_index=diag_index, lam=lam)
+    for s in range(nsys):
+        ref = O.sense_normal_toeplitz(xs[s], sm, Ts[diag_index[s]], coils) + lam * xs[s]
+        assert O.rel_l2(_np(out[s]), ref) < TOL
+
+
+def test_sense_normal_workspace_groups(cuda):
+    """A workspace too small for all systems at once: processed in groups, same result."""
+    shape = (16, 16, 16)
+    plan = ToeplitzPlan(shape, cuda)
+    sm = _c64(synth.coil_maps(4, shape, seed=6), cuda)
+    T = O.toeplitz_diagonal(np.random.default_rng(1).uniform(-np.pi, np.pi, (3, 300)), shape)
+    packed = plan.pack_diagonal(_c64(T, cuda))
+    xs = _c64(np.stack([synth.gaussian_image(shape, seed=s) for s in range(5)]), cuda)
+    full = torch.empty_like(xs)
+    plan.sense_normal(xs, full, sm, packed)
+    part = torch.empty_like(xs)
+    nb = capi.load().hb_normal_workspace_bytes(plan._h, 2, 4)
+    plan._ws = None
+    plan.sense_normal(xs, part, sm, packed, workspace_bytes=nb)
+    assert torch.equal(full, part)
+
+
+def test_config1_size_normal_op(cuda):
+    """64^3, 8 coils (the CPU-runnable configuration's size) against the FP64 oracle."""
+    shape = (64, 64, 64)
+    rng = np.random.default_rng(14)
+    plan = ToeplitzPlan(shape, cuda)
+    coords = synth.kooshball(256, 128)
+    packed, Tg = plan.build_diagonal(torch.from_numpy(coords), want_complex=True)
+    T = _np(Tg)  # reference-layout diagonal from the GPU FP64 builder (checked separately)
+    sm = synth.coil_maps(8, shape, seed=7)
+    x = synth.gaussian_image(shape, seed=8)
+    out = torch.empty(shape, dtype=torch.complex64, device=cuda)
+    plan.sense_normal(_c64(x, cuda), out, _c64(sm, cuda), packed)
+    ref = O.sense_normal_toeplitz(x, sm, T)
+    assert O.rel_l2(_np(out), ref) < TOL
+
+
+def test_large_size_properties(cuda):
+    """128^3 x 16 coils: Hermitian (<Ax,y> = <x,Ay>), linearity, bitwise determinism."""
+    shape = (128, 128, 128)
+    plan = ToeplitzPlan(shape, cuda)
+    coords = synth.kooshball(400, 256)
+    packed = plan.build_diagonal(torch.from_numpy(coords))
+    sm = _c64(synth.coil_maps(16, shape, seed=9), cuda)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    xs = torch.randn((2,) + shape, dtype=torch.complex64, generator=g).to(cuda)
+    out = torch.empty_like(xs)
+    plan.sense_normal(xs, out, sm, packed)
+    ax, ay = out[0].double(), out[1].double()
+    x, y = xs[0].double(), xs[1].double()
+    lhs = torch.vdot(ax.flatten(), y.flatten())
+    rhs = torch.vdot(x.flatten(), ay.flatten())
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+    assert torch.vdot(x.flatten(), ax.flatten()).real > 0
+    # linearity
+    comb = (xs[0] * (0.5 - 0.25j) + xs[1] * 2.0).unsqueeze(0).contiguous()
+    oc = torch.empty_like(comb)
+    plan.sense_normal(comb, oc, sm, packed)
+    lin = out[0] * (0.5 - 0.25j) + out[1] * 2.0
+    assert (torch.linalg.vector_norm(oc[0] - lin) / torch.linalg.vector_norm(lin)).item() < 1e-5
+    # determinism
+    out2 = torch.empty_like(xs)
+    plan.sense_normal(xs, out2, sm, packed)
+    assert torch.equal(out, out2)
+
+
+@pytest.mark.parametrize("shape,ncoil,nsys", [((16, 16, 16), 4, 3), ((32, 32, 32), 8, 2)])
+def test_cg_matches_oracle(cuda, shape, ncoil, nsys):
+    rng = np.random.default_rng(15)
+    plan = ToeplitzPlan(shape, cuda)
+    sm = synth.coil_maps(ncoil, shape, seed=10)
+    Ts = [O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 2000)), shape) for _ in range(2)]
+    packed = torch.cat([plan.pack_diagonal(_c64(T, cuda)) for T in Ts])
+    diag_index = [s % 2 for s in range(nsys)]
+    lam = 1e-3
+    iters = 10
+    xtrue = np.stack([synth.gaussian_image(shape, seed=30 + s) for s in range(nsys)])
+    bs = np.stack([O.sense_normal_toeplitz(xtrue[s], sm, Ts[diag_index[s]]) + lam * xtrue[s] for s in range(nsys)])
+    xg = torch.zeros((nsys,) + shape, dtype=torch.complex64, device=cuda)
+    status, done = plan.cg(xg, _c64(bs, cuda), _c64(sm, cuda), packed, iters=iters, lam=lam, diag_index=diag_index)
+    assert status == [capi.HB_CG_RUNNING] * nsys and done == [iters] * nsys
+    for s in range(nsys):
+        A = O.regularized(lambda v, s=s: O.sense_normal_toeplitz(v, sm, Ts[diag_index[s]]), lam)
+        xo, n = O.conjugate_gradient(A, bs[s], iters=iters)
+        assert O.rel_l2(_np(xg[s]), xo) < 1e-4  # FP32 vectors over 10 iterations
+
+
+def test_cg_tol_stops_early(cuda):
+    shape = (16, 16, 16)
+    plan = ToeplitzPlan(shape, cuda)
+    sm = _c64(synth.coil_maps(2, shape, seed=1), cuda)
+    T = np.ones(plan.grid, np.complex128)  # identity normal op: sum_c |S_c|^2 = 1
+    packed = plan.pack_diagonal(_c64(T, cuda))
+    b = _c64(synth.gaussian_image(shape, seed=2), cuda)
+    x = torch.zeros_like(b)
+    status, done = plan.cg(x, b, sm, packed, iters=20, tol=1e-3)
+    assert status == [capi.HB_CG_CONVERGED]
+    assert done[0] <= 2
+    assert (torch.linalg.vector_norm(x - b) / torch.linalg.vector_norm(b)).item() < 1e-5
+
+
+def test_cg_not_positive_definite(cuda):
+    """A host-made fault: a negated diagonal makes A negative definite; the device flags
+    the system and the call raises like the reference ("A was not positive definite")."""
+    shape = (16, 16, 16)
+    plan = ToeplitzPlan(shape, cuda)
+    sm = _c64(synth.coil_maps(2, shape, seed=1), cuda)
+    T = -np.ones(plan.grid, np.complex128)
+    packed = plan.pack_diagonal(_c64(T, cuda))
+    b = _c64(synth.gaussian_image(shape, seed=2), cuda)
+    x = torch.zeros_like(b)
+    with pytest.raises(capi.NotPositiveDefinite):
+        plan.cg(x, b, sm, packed, iters=5)
+    status, done = plan.cg(torch.zeros_like(b), b, sm, packed, iters=5, raise_not_pd=False)
+    assert status == [capi.HB_CG_NOT_PD] and done == [0]
+
+
+def test_invalid_arguments_raise(cuda):
+    with pytest.raises(capi.HastyError):
+        ToeplitzPlan((12, 16, 16), cuda)
+    plan = ToeplitzPlan((8, 8, 8), cuda)
+    with pytest.raises(RuntimeError):
+        plan.pack_diagonal(torch.zeros((16, 16, 16), dtype=torch.complex128, device=cuda))
+    lib = capi.load()
+    assert lib.hb_toeplitz_apply(plan._h, None, None, 0, 0, None, 0, None, None, 0, None) == capi.HB_ERR_INVALID
+    assert b"NULL" in lib.hb_last_error()

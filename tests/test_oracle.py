@@ -1,0 +1,122 @@
+"""CPU tests of the FP64 oracle: pinned to the reference's own code and known answers."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_ahwa.npz")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(GOLDEN)
+
+
+@pytest.mark.parametrize("case", ["cnm", "rnd"])
+def test_toeplitz_matches_reference_dense_builder(golden, case):
+    """Oracle Toeplitz op x prod(2N) == the reference's dense A^H W A
+    (toep_builder.py compute_AHWA, executed from the reference source by make_golden.py)."""
+    x = golden[f"x_{case}"]
+    y = golden[f"y_{case}"]
+    nf = int(golden[f"nf_{case}"])
+    c = golden["coords"][:, :nf].astype(np.float64)
+    T = O.toeplitz_diagonal(c, x.shape)
+    got = O.toeplitz_apply(x, T) * np.prod(O.grid2(x.shape))
+    assert O.rel_l2(got, y) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["cnm", "rnd"])
+def test_explicit_normal_matches_reference_dense_builder(golden, case):
+    x = golden[f"x_{case}"]
+    y = golden[f"y_{case}"]
+    nf = int(golden[f"nf_{case}"])
+    c = golden["coords"][:, :nf].astype(np.float64)
+    got = O.explicit_normal(x, c) * np.prod(x.shape)
+    assert O.rel_l2(got, y) < 1e-12
+
+
+def test_explicit_over_toeplitz_is_eight(golden):
+    """compare_normal_methods (tests1.cpp:351-549): explicit normal / Toeplitz = 2^3."""
+    x = golden["x_cnm"]
+    c = golden["coords"][:, :30].astype(np.float64)
+    T = O.toeplitz_diagonal(c, x.shape)
+    ratio = O.explicit_normal(x, c) / O.toeplitz_apply(x, T)
+    assert np.allclose(ratio, 8.0, rtol=1e-10, atol=0)
+
+
+def test_real_part_of_diagonal_suffices():
+    rng = np.random.default_rng(3)
+    N = (6, 4, 8)
+    c = rng.uniform(-np.pi, np.pi, (3, 400))
+    T = O.toeplitz_diagonal(c, N)
+    assert np.abs(T.imag).max() > 1e-3 * np.abs(T).max()  # Im(T) is not negligible ...
+    x = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    a = O.toeplitz_apply(x, T)
+    b = O.toeplitz_apply(x, T.real.astype(np.complex128))
+    assert O.rel_l2(b, a) < 1e-13  # ... but it never reaches the cropped output
+
+
+def test_diagonal_build_matches_impulse_construction():
+    """nufft.cpp:932-971 literally: impulse at M/2, normal op on the 2x grid, ifftshift, fftn."""
+    rng = np.random.default_rng(4)
+    N = (4, 6, 4)
+    M = O.grid2(N)
+    c = rng.uniform(-np.pi, np.pi, (3, 50))
+    delta = np.zeros(M, np.complex128)
+    delta[M[0] // 2, M[1] // 2, M[2] // 2] = 1.0
+    normal = O.explicit_normal(delta, c) * np.prod(M) / np.prod(M)  # explicit on the M grid: /prod(M)
+    T_imp = np.fft.fftn(np.fft.ifftshift(normal))
+    T = O.toeplitz_diagonal(c, N)
+    assert O.rel_l2(T, T_imp) < 1e-12
+
+
+def _dense(op, shape):
+    n = int(np.prod(shape))
+    A = np.zeros((n, n), np.complex128)
+    for j in range(n):
+        e = np.zeros(n, np.complex128)
+        e[j] = 1
+        A[:, j] = op(e.reshape(shape)).ravel()
+    return A
+
+
+def test_sense_normal_dense_hermitian_psd():
+    rng = np.random.default_rng(5)
+    N = (4, 4, 4)
+    c = rng.uniform(-np.pi, np.pi, (3, 300))
+    T = O.toeplitz_diagonal(c, N)
+    sm = rng.standard_normal((3,) + N) + 1j * rng.standard_normal((3,) + N)
+    A = _dense(lambda v: O.sense_normal_toeplitz(v, sm, T), N)
+    assert np.allclose(A, A.conj().T, atol=1e-10 * np.abs(A).max())
+    assert np.linalg.eigvalsh(A).min() > -1e-9 * np.abs(A).max()
+
+
+def test_cg_matches_direct_solve():
+    rng = np.random.default_rng(6)
+    N = (4, 4, 4)
+    c = rng.uniform(-np.pi, np.pi, (3, 500))
+    T = O.toeplitz_diagonal(c, N)
+    sm = rng.standard_normal((2,) + N) + 1j * rng.standard_normal((2,) + N)
+    lam = 1e-1
+    op = O.regularized(lambda v: O.sense_normal_toeplitz(v, sm, T), lam)
+    A = _dense(op, N)
+    b = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    x_direct = np.linalg.solve(A, b.ravel()).reshape(N)
+    x, n = O.conjugate_gradient(op, b, iters=200, tol=1e-12)
+    assert O.rel_l2(x, x_direct) < 1e-8
+
+
+def test_cg_not_positive_definite_raises():
+    b = np.ones((2, 2, 2), np.complex128)
+    with pytest.raises(O.NotPositiveDefinite):
+        O.conjugate_gradient(lambda v: -v, b, iters=3)
+
+
+def test_cg_tol_and_iter_zero():
+    b = np.ones((2, 2, 2), np.complex128)
+    x, n = O.conjugate_gradient(lambda v: 2 * v, b, iters=0)
+    assert n == 0 and np.all(x == 0)
+    x, n = O.conjugate_gradient(lambda v: 2 * v, b, iters=10, tol=1e-9)
+    assert n == 1 and np.allclose(x, 0.5)
