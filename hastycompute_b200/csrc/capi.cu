@@ -388,9 +388,14 @@ int hb_diag_build(const hb_plan* p, const float* coords, int64_t nsamples, float
                                                                              (double2*)tabs[ax]);
       HB_CHECK_LAUNCH();
     }
-    dim3 grid((M2 + kDiagTile - 1) / kDiagTile, (M1 + kDiagTile - 1) / kDiagTile, M0);
     LaunchScope ls(HB_KERNEL_DIAG, st);
-    diag_accumulate_kernel<<<grid, 256, 0, st>>>(Dz, Dy, Dx, nj, M0, M1, M2, acc);
+    if (T_complex) {
+      dim3 grid((M2 + kDiagTileX - 1) / kDiagTileX, (M1 + 63) / 64, M0);
+      diag_accumulate_kernel<true, 4><<<grid, 256, 0, st>>>(Dz, Dy, Dx, nj, M0, M1, M2, acc);
+    } else {
+      dim3 grid((M2 + kDiagTileX - 1) / kDiagTileX, (M1 + 127) / 128, M0);
+      diag_accumulate_kernel<false, 8><<<grid, 256, 0, st>>>(Dz, Dy, Dx, nj, M0, M1, M2, acc);
+    }
     HB_CHECK_LAUNCH();
   }
   const double psf_scale = 1.0 / (double)n;

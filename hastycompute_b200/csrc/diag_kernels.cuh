@@ -44,62 +44,67 @@ __global__ void dirichlet_table_kernel(const float* __restrict__ c, long long j0
   D[idx] = make_double2(re, im);
 }
 
-// acc[kz][ky][kx] += sum_j Dz[j][kz] * Dy[j][ky] * Dx[j][kx]   (complex, FP64)
-// grid: (M2/64, M1/64, M0), block 256 = 16 x 16 lanes, each lane a 4 x 4 (ky, kx) tile.
-constexpr int kDiagTile = 64;
+// acc[kz][ky][kx] += sum_j Dz[j][kz] * Dy[j][ky] * Dx[j][kx]   (FP64)
+// CPLX: the full complex sum; otherwise only its real part (half the FMAs), which is all
+// the normal operator reads.  grid: (ceil(M2/64), ceil(M1/(16*TI)), M0), block 16 x 16
+// lanes, each lane a TI x 4 (ky, kx) register tile.
+constexpr int kDiagTileX = 64;
 constexpr int kDiagJB = 16;
 
+template <bool CPLX, int TI>
 __global__ void __launch_bounds__(256)
 diag_accumulate_kernel(const double2* __restrict__ Dz, const double2* __restrict__ Dy,
                        const double2* __restrict__ Dx, int nj, int M0, int M1, int M2,
                        double2* __restrict__ acc) {
-  __shared__ double2 As[kDiagJB][kDiagTile];
-  __shared__ double2 Bs[kDiagJB][kDiagTile];
-  const int kx0 = blockIdx.x * kDiagTile, ky0 = blockIdx.y * kDiagTile, kz = blockIdx.z;
+  constexpr int TY = 16 * TI;
+  __shared__ double2 As[kDiagJB][TY];
+  __shared__ double2 Bs[kDiagJB][kDiagTileX];
+  const int kx0 = blockIdx.x * kDiagTileX, ky0 = blockIdx.y * TY, kz = blockIdx.z;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double2 r[4][4];
+  double2 r[TI][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < TI; ++i)
 #pragma unroll
     for (int m = 0; m < 4; ++m) r[i][m] = make_double2(0.0, 0.0);
 
   for (int jb = 0; jb < nj; jb += kDiagJB) {
     __syncthreads();
-    for (int i = threadIdx.x; i < kDiagJB * kDiagTile; i += 256) {
-      const int jl = i / kDiagTile, q = i % kDiagTile;
+    for (int i = threadIdx.x; i < kDiagJB * TY; i += 256) {
+      const int jl = i / TY, q = i % TY;
       const int j = jb + jl;
-      double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
-      if (j < nj) {
+      double2 a = make_double2(0.0, 0.0);
+      const int ky = ky0 + q;
+      if (j < nj && ky < M1) {
         const double2 dz = Dz[(long long)j * M0 + kz];
-        const int ky = ky0 + q, kx = kx0 + q;
-        if (ky < M1) {
-          const double2 dy = Dy[(long long)j * M1 + ky];
-          a = make_double2(dz.x * dy.x - dz.y * dy.y, dz.x * dy.y + dz.y * dy.x);
-        }
-        if (kx < M2) b = Dx[(long long)j * M2 + kx];
+        const double2 dy = Dy[(long long)j * M1 + ky];
+        a = make_double2(dz.x * dy.x - dz.y * dy.y, dz.x * dy.y + dz.y * dy.x);
       }
       As[jl][q] = a;
-      Bs[jl][q] = b;
+    }
+    for (int i = threadIdx.x; i < kDiagJB * kDiagTileX; i += 256) {
+      const int jl = i / kDiagTileX, q = i % kDiagTileX;
+      const int j = jb + jl, kx = kx0 + q;
+      Bs[jl][q] = (j < nj && kx < M2) ? Dx[(long long)j * M2 + kx] : make_double2(0.0, 0.0);
     }
     __syncthreads();
 #pragma unroll 4
     for (int jl = 0; jl < kDiagJB; ++jl) {
-      double2 av[4], bv[4];
+      double2 av[TI], bv[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = As[jl][ty + 16 * i];
+      for (int i = 0; i < TI; ++i) av[i] = As[jl][ty + 16 * i];
 #pragma unroll
       for (int m = 0; m < 4; ++m) bv[m] = Bs[jl][tx + 16 * m];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < TI; ++i)
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           r[i][m].x = fma(av[i].x, bv[m].x, fma(-av[i].y, bv[m].y, r[i][m].x));
-          r[i][m].y = fma(av[i].x, bv[m].y, fma(av[i].y, bv[m].x, r[i][m].y));
+          if (CPLX) r[i][m].y = fma(av[i].x, bv[m].y, fma(av[i].y, bv[m].x, r[i][m].y));
         }
     }
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < TI; ++i) {
     const int ky = ky0 + ty + 16 * i;
     if (ky >= M1) continue;
 #pragma unroll
@@ -109,7 +114,7 @@ diag_accumulate_kernel(const double2* __restrict__ Dz, const double2* __restrict
       double2* p = acc + ((long long)kz * M1 + ky) * M2 + kx;
       double2 v = *p;
       v.x += r[i][m].x;
-      v.y += r[i][m].y;
+      if (CPLX) v.y += r[i][m].y;
       *p = v;
     }
   }

@@ -56,7 +56,7 @@ def coil_maps(ncoil, shape, seed=0, dtype=np.complex64):
 
 def gaussian_image(shape, seed=0, dtype=np.complex64):
     rng = np.random.default_rng(seed)
-    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype) / np.sqrt(2.0)
+    return ((rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) / np.sqrt(2.0)).astype(dtype)
 
 
 def flow_phantom(shape, nenc, seed=0, noise=1e-3, dtype=np.complex64):

@@ -68,6 +68,8 @@ def test_diagonal_build_fp64(cuda, shape):
     assert O.rel_l2(_np(Tg), T) < 1e-6
     packed_ref = plan.pack_diagonal(_c64(T, cuda))
     assert O.rel_l2(packed.cpu().numpy(), packed_ref.cpu().numpy()) < 1e-6
+    packed_real_only = plan.build_diagonal(torch.from_numpy(coords))  # Re(T) accumulation only
+    assert O.rel_l2(packed_real_only.cpu().numpy(), packed_ref.cpu().numpy()) < 1e-6
 
 
 def test_diagonal_build_on_grid_samples(cuda):
@@ -144,8 +146,8 @@ def test_large_size_properties(cuda):
     xs = torch.randn((2,) + shape, dtype=torch.complex64, generator=g).to(cuda)
     out = torch.empty_like(xs)
     plan.sense_normal(xs, out, sm, packed)
-    ax, ay = out[0].double(), out[1].double()
-    x, y = xs[0].double(), xs[1].double()
+    ax, ay = out[0].to(torch.complex128), out[1].to(torch.complex128)
+    x, y = xs[0].to(torch.complex128), xs[1].to(torch.complex128)
     lhs = torch.vdot(ax.flatten(), y.flatten())
     rhs = torch.vdot(x.flatten(), ay.flatten())
     assert abs(lhs - rhs) / abs(lhs) < 1e-5

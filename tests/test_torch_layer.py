@@ -1,0 +1,111 @@
+"""GPU tests of the C++/LibTorch host layer and its TorchScript classes against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from hastycompute_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def ffi(cuda):
+    from hastycompute_b200.ffi import hasty_toeplitz
+
+    return hasty_toeplitz
+
+
+def _np(t):
+    return t.detach().cpu().numpy().astype(np.complex128)
+
+
+def test_normal_nufft_toeplitz_from_coords(ffi, cuda):
+    shape = (16, 8, 16)
+    rng = np.random.default_rng(0)
+    coords = torch.from_numpy(rng.uniform(-np.pi, np.pi, (3, 500)).astype(np.float32)).to(cuda)
+    op = ffi.NormalNufftToeplitz(coords, [1, *shape])
+    T = O.toeplitz_diagonal(coords.cpu().numpy().astype(np.float64), shape)
+    assert O.rel_l2(_np(op.get_diagonal()[0]), T) < 1e-6
+    x = torch.from_numpy(synth.gaussian_image((1,) + shape, seed=1)).to(cuda)
+    M = tuple(2 * n for n in shape)
+    s1 = torch.empty((1,) + M, dtype=torch.complex64, device=cuda)
+    s2 = torch.empty_like(s1)
+    y = op.apply(x, s1, s2)
+    ref = O.toeplitz_apply(_np(x[0]), T)
+    assert y.shape == (1,) + shape
+    assert y.data_ptr() == s2.data_ptr()  # a view into storage2, as in the reference
+    assert O.rel_l2(_np(y[0]), ref) < TOL
+    add = torch.ones_like(x)
+    mul = torch.from_numpy(synth.gaussian_image((1,) + shape, seed=2)).to(cuda)
+    op.apply_addcmul(x, add, mul, s1, s2)
+    assert O.rel_l2(_np(add[0]), 1 + ref * _np(mul[0])) < TOL
+    xi = x.clone()
+    op.apply_inplace(xi, s1, s2)
+    assert O.rel_l2(_np(xi[0]), ref) < TOL
+
+
+def test_sense_normal_toeplitz_from_diagonal(ffi, cuda):
+    shape = (16, 16, 16)
+    rng = np.random.default_rng(1)
+    T = O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 700)), shape)
+    sm = synth.coil_maps(4, shape, seed=3)
+    x = synth.gaussian_image((1,) + shape, seed=4)
+    op = ffi.SenseNormalToeplitz(None, [1, *shape], torch.from_numpy(T.astype(np.complex64)).reshape(1, 32, 32, 32).to(cuda))
+    out = torch.empty((1,) + shape, dtype=torch.complex64, device=cuda)
+    coils = [3, 1, 2]
+    op.apply(torch.from_numpy(x).to(cuda), out, torch.from_numpy(sm).to(cuda), coils)
+    ref = O.sense_normal_toeplitz(x[0], sm, T, coils)
+    assert O.rel_l2(_np(out[0]), ref) < TOL
+
+
+def test_batched_sense_cpu_tensors_and_cg(ffi, cuda):
+    shape = (16, 16, 16)
+    rng = np.random.default_rng(2)
+    Ts = [O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 1500)), shape) for _ in range(2)]
+    diags = torch.from_numpy(np.stack(Ts).astype(np.complex64))
+    sm = synth.coil_maps(3, shape, seed=5)
+    nouter = 3
+    didx = [1, 0, 1]
+    op = ffi.BatchedSenseNormalToeplitz(diags, torch.from_numpy(sm), didx)
+    x = torch.from_numpy(np.stack([synth.gaussian_image((1,) + shape, seed=10 + i) for i in range(nouter)]))
+    out = torch.empty_like(x)  # CPU tensors, as the reference's batched operators take
+    op.apply(x, out, [[0, 1, 2], [2], [0, 1, 2]])
+    for i, cl in enumerate([[0, 1, 2], [2], [0, 1, 2]]):
+        ref = O.sense_normal_toeplitz(x[i, 0].numpy(), sm, Ts[didx[i]], cl)
+        assert O.rel_l2(out[i, 0].numpy(), ref) < TOL
+    # CG through the TorchScript class
+    lam = 1e-3
+    b = torch.empty_like(x)
+    op.apply(x, b, None, lam)
+    xs = torch.zeros_like(x).to(cuda)
+    iters = op.cg(xs, b.to(cuda), 8, 0.0, lam, None)
+    assert list(iters) == [8] * nouter
+    for i in range(nouter):
+        A = O.regularized(lambda v, i=i: O.sense_normal_toeplitz(v, sm, Ts[didx[i]]), lam)
+        xo, _ = O.conjugate_gradient(A, b[i, 0].numpy().astype(np.complex128), iters=8)
+        assert O.rel_l2(_np(xs[i, 0]), xo) < 1e-4
+
+
+def test_legacy_batched_binding_in_place(ffi, cuda):
+    shape = (8, 8, 8)
+    rng = np.random.default_rng(3)
+    Ts = [O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 300)), shape) for _ in range(2)]
+    sm = synth.coil_maps(2, shape, seed=6)
+    x = np.stack([synth.gaussian_image((1,) + shape, seed=20 + i) for i in range(2)])
+    xt = torch.from_numpy(x.copy())
+    ffi.batched_sense_toeplitz_diagonals(xt, [[0, 1], [0, 1]], torch.from_numpy(sm),
+                                         torch.from_numpy(np.stack(Ts).astype(np.complex64)))
+    for i in range(2):
+        assert O.rel_l2(xt[i, 0].numpy(), O.sense_normal_toeplitz(x[i, 0], sm, Ts[i])) < TOL
+
+
+def test_errors_are_runtime_errors(ffi, cuda):
+    with pytest.raises(RuntimeError, match="not supported"):
+        ffi.SenseNormalToeplitz(None, [1, 12, 16, 16], torch.zeros((1, 24, 32, 32), dtype=torch.complex64, device=cuda))
+    op = ffi.SenseNormalToeplitz(None, [1, 8, 8, 8], torch.ones((1, 16, 16, 16), dtype=torch.complex64, device=cuda))
+    x = torch.zeros((1, 8, 8, 8), dtype=torch.complex64, device=cuda)
+    sm = torch.ones((2, 8, 8, 8), dtype=torch.complex64, device=cuda)
+    with pytest.raises(RuntimeError, match="coil index"):
+        op.apply(x, torch.empty_like(x), sm, [0, 5])
