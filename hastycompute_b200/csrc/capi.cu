@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -149,7 +150,7 @@ cudaError_t launch_a(const PassArgs& a, int nslots, cudaStream_t st) {
 template <int N2, int YT>
 cudaError_t launch_c(const PassArgs& a, int nsys, cudaStream_t st) {
   using C = XPassCfg<N2, YT>;
-  const size_t smem = C::SMEM_F2 * sizeof(float2);
+  const size_t smem = C::SMEM_F2_C * sizeof(float2);
   cudaError_t e = ensure_smem(inv_x_combine_kernel<N2, YT>, smem);
   if (e != cudaSuccess) return e;
   dim3 grid(a.N1 / YT, a.N0, nsys);
@@ -158,28 +159,68 @@ cudaError_t launch_c(const PassArgs& a, int nsys, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <int N0, int N1>
+template <int N0, int N1, int Q, int THREADS>
 cudaError_t launch_b(const PassArgs& a, int nslots, cudaStream_t st) {
-  using C = PlaneCfg<N0, N1>;
+  using C = PlaneCfg<N0, N1, Q, THREADS>;
   const size_t smem = C::SMEM_F2 * sizeof(float2);
-  cudaError_t e = ensure_smem(plane_yz_kernel<N0, N1>, smem);
+  cudaError_t e = ensure_smem(plane_yz_kernel<N0, N1, Q, THREADS>, smem);
   if (e != cudaSuccess) return e;
-  dim3 grid(2, nslots, 2 * a.N2);
+  dim3 grid(2 * Q, nslots, 2 * a.N2);
+  PassArgs b = a;
+  // one wave of clusters ahead: co-resident clusters = SMs * (CTAs per SM) / (2Q)
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const int per_sm = (int)((227 * 1024) / (smem + 1024));
+  b.prefetch_ahead = getenv("HB_NO_L2_PREFETCH") ? 0 : sms * (per_sm < 1 ? 1 : per_sm) / (2 * Q);
   LaunchScope ls(HB_KERNEL_PLANE_YZ, st);
-  plane_yz_kernel<N0, N1><<<grid, C::THREADS, smem, st>>>(a);
+  plane_yz_kernel<N0, N1, Q, THREADS><<<grid, THREADS, smem, st>>>(b);
   return cudaGetLastError();
 }
 
+// Plane-pass variants for the large planes (selected by HB_PLANE_VARIANT for tuning)
+struct PlaneVariant {
+  const char* name;
+  PassLauncher fn;
+};
+const PlaneVariant kPlane128[] = {
+    {"q1t512", &launch_b<128, 128, 1, 512>}, {"q2t256", &launch_b<128, 128, 2, 256>},
+    {"q2t128", &launch_b<128, 128, 2, 128>}, {"q4t256", &launch_b<128, 128, 4, 256>},
+    {"q4t128", &launch_b<128, 128, 4, 128>},
+};
+const PlaneVariant kPlane64[] = {
+    {"q1t256", &launch_b<64, 64, 1, 256>}, {"q2t128", &launch_b<64, 64, 2, 128>},
+    {"q1t128", &launch_b<64, 64, 1, 128>}, {"q2t256", &launch_b<64, 64, 2, 256>},
+};
+
+int plane_variant_index(int nvariants) {
+  const char* env = getenv("HB_PLANE_VARIANT");
+  if (!env) return 0;
+  int v = atoi(env);
+  return (v >= 0 && v < nvariants) ? v : 0;
+}
+
 // [log2(N2)-3][log2(YT)-3]
-#define HB_XROW(N2, F) {&F<N2, 8>, &F<N2, 16>, &F<N2, 32>}
-const PassLauncher kLaunchA[5][3] = {HB_XROW(8, launch_a), HB_XROW(16, launch_a), HB_XROW(32, launch_a),
+#define HB_XROW(N2, F) {&F<N2, 8>, &F<N2, 16>}
+const PassLauncher kLaunchA[5][2] = {HB_XROW(8, launch_a), HB_XROW(16, launch_a), HB_XROW(32, launch_a),
                                      HB_XROW(64, launch_a), HB_XROW(128, launch_a)};
-const PassLauncher kLaunchC[5][3] = {HB_XROW(8, launch_c), HB_XROW(16, launch_c), HB_XROW(32, launch_c),
+const PassLauncher kLaunchC[5][2] = {HB_XROW(8, launch_c), HB_XROW(16, launch_c), HB_XROW(32, launch_c),
                                      HB_XROW(64, launch_c), HB_XROW(128, launch_c)};
-#define HB_BROW(N0) {&launch_b<N0, 8>, &launch_b<N0, 16>, &launch_b<N0, 32>, &launch_b<N0, 64>, &launch_b<N0, 128>}
+#define HB_BROW(N0)                                                                                    \
+  {&launch_b<N0, 8, 1, 128>, &launch_b<N0, 16, 1, 128>, &launch_b<N0, 32, 1, 128>, &launch_b<N0, 64, 1, 256>, \
+   &launch_b<N0, 128, 1, 512>}
 const PassLauncher kLaunchB[5][5] = {HB_BROW(8), HB_BROW(16), HB_BROW(32), HB_BROW(64), HB_BROW(128)};
 
-int yt_for(int N1) { return N1 < 32 ? N1 : 32; }
+PassLauncher plane_launcher(int N0, int N1) {
+  if (N0 == 128 && N1 == 128) return kPlane128[plane_variant_index(5)].fn;
+  if (N0 == 64 && N1 == 64) return kPlane64[plane_variant_index(4)].fn;
+  return kLaunchB[ilog2(N0) - 3][ilog2(N1) - 3];
+}
+
+int yt_for(int N1) { return N1 < 16 ? N1 : 16; }
 
 // Runs passes A, B, C for `nsys` systems described by `a`.
 int run_normal(const hb_plan* p, PassArgs a, cudaStream_t st) {
@@ -189,7 +230,7 @@ int run_normal(const hb_plan* p, PassArgs a, cudaStream_t st) {
   if (nslots > 65535) return fail(HB_ERR_INVALID, "too many system x coil slots in one launch (max 65535)");
   cudaError_t e = kLaunchA[ia][iy](a, nslots, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass A: ") + cudaGetErrorString(e));
-  e = kLaunchB[ilog2(p->N0) - 3][ilog2(p->N1) - 3](a, nslots, st);
+  e = plane_launcher(p->N0, p->N1)(a, nslots, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass B: ") + cudaGetErrorString(e));
   e = kLaunchC[ia][iy](a, a.nsys, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass C: ") + cudaGetErrorString(e));

@@ -29,4 +29,15 @@ HB_DEV float2 crot(float2 a, float c, float s) {
   return make_float2(fmaf(a.x, c, -a.y * s), fmaf(a.x, s, a.y * c));
 }
 
+// ---- asynchronous global -> shared copies (cp.async, completion by groups) ----
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 }  // namespace hb

@@ -214,6 +214,65 @@ __device__ __forceinline__ void team_fft_dout_to_din(float2* v, int t, float2* b
   (void)HALF_OUT;  // unused outputs are removed by dead-code elimination
 }
 
+// Variants with this lane's twiddles held in registers: twr[k1] = tw[k1*S + t]
+// (forward sign).  Lane t's twiddles never change, so kernels that run many lines of
+// the same length load them once.
+template <int L>
+__device__ __forceinline__ void load_lane_twiddles(float2* twr, const float2* tw, int t) {
+  constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) twr[k1] = tw[k1 * S + t];
+}
+
+template <int L, int DIR, bool HALF_IN>
+__device__ __forceinline__ void team_fft_din_to_dout_r(float2* v, int t, float2* buf, const float2* twr) {
+  constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+  if constexpr (HALF_IN) DftHalfIn<E, DIR>::run(v);
+  else Dft<E, DIR>::run(v);
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) {
+    float2 w = twr[k1];
+    if (DIR > 0) w.y = -w.y;
+    buf[k1 * (S + 1) + t] = k1 == 0 ? v[0] : cmul(v[k1], w);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < E / S; ++c) {
+    float2 u[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) u[j] = buf[(t + S * c) * (S + 1) + j];
+    Dft<S, DIR>::run(u);
+#pragma unroll
+    for (int k2 = 0; k2 < S; ++k2) v[c * S + k2] = u[k2];
+  }
+  __syncwarp();
+}
+
+template <int L, int DIR, bool HALF_OUT>
+__device__ __forceinline__ void team_fft_dout_to_din_r(float2* v, int t, float2* buf, const float2* twr) {
+  constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+#pragma unroll
+  for (int c = 0; c < E / S; ++c) {
+    float2 u[S];
+#pragma unroll
+    for (int k2 = 0; k2 < S; ++k2) u[k2] = v[c * S + k2];
+    Dft<S, DIR>::run(u);
+#pragma unroll
+    for (int j = 0; j < S; ++j) buf[(t + S * c) * (S + 1) + j] = u[j];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) {
+    float2 w = twr[k1];
+    if (DIR > 0) w.y = -w.y;
+    const float2 b = buf[k1 * (S + 1) + t];
+    v[k1] = k1 == 0 ? b : cmul(b, w);
+  }
+  __syncwarp();
+  Dft<E, DIR>::run(v);
+  (void)HALF_OUT;
+}
+
 // Index helpers for the two layouts.
 template <int L>
 HB_DEV int din_index(int t, int e) { return t + TeamCfg<L>::S * e; }

@@ -39,26 +39,50 @@ struct XPassCfg {
   static constexpr int NTEAMS = THREADS / S;
   static constexpr int TILE_LD = YT + 1;  // padded row of the [kx][y] staging tile
   static constexpr int TBUF = team_buf_stride<M2>();
-  // float2 slots of dynamic shared memory
+  // float2 slots of dynamic shared memory: pass A stages one [kx][y] tile, pass C
+  // double-buffers the tiles of consecutive coils
   static constexpr int SMEM_F2 = M2 * TILE_LD + NTEAMS * TBUF + M2;
+  static constexpr int SMEM_F2_C = 2 * M2 * TILE_LD + NTEAMS * TBUF + M2;
   static_assert(THREADS % 32 == 0, "x-pass CTA must be whole warps");
 };
 
-// Pass B: a CTA of THREADS lanes owns an N0 x N1 plane (one ky-parity half).
-template <int N0, int N1>
+// Row handled by team j of a row stage: the teams sharing a half-warp take rows S apart,
+// so their (odd-pitch) plane rows start on disjoint shared-memory banks.
+template <int S, int NTEAMS, int ROWS>
+__device__ __forceinline__ int row_of_team(int j) {
+  constexpr int TPH = S < 16 ? 16 / S : 1;
+  if constexpr (TPH > 1 && NTEAMS % 16 == 0 && ROWS % 16 == 0) {
+    return (j / 16) * 16 + (j % TPH) * S + (j / TPH) % S;
+  } else {
+    return j;
+  }
+}
+
+// Pass B: a cluster of 2*Q CTAs owns one N0 x N1 (z, y) plane.  CTA rank r = h*Q + q
+// handles ky parity h; for the z-FFTs it owns the ky' columns [q*H, (q+1)*H) (H = N1/Q),
+// for the y-FFTs the rows [q*ZR, (q+1)*ZR) (ZR = N0/Q).  Rows and columns meet through
+// distributed shared memory.
+template <int N0, int N1, int Q, int THREADS_>
 struct PlaneCfg {
   static constexpr int M0 = 2 * N0;
-  static constexpr int THREADS = (N0 * N1 >= 4096) ? 512 : 128;
+  static constexpr int THREADS = THREADS_;
   static constexpr int SR = TeamCfg<N1>::S, ER = TeamCfg<N1>::E;
   static constexpr int SZ = TeamCfg<M0>::S, EZ = TeamCfg<M0>::E;
+  static constexpr int H = N1 / Q;    // owned columns (z stage)
+  static constexpr int ZR = N0 / Q;   // owned rows (y stages)
   static constexpr int NTEAMS_R = THREADS / SR;
   static constexpr int NTEAMS_Z = THREADS / SZ;
-  static constexpr int LD = N1 + 1;  // padded plane row
+  static constexpr int LPT_R = (ZR + NTEAMS_R - 1) / NTEAMS_R;  // rows per team
+  static constexpr int LDP = H + 1;   // column-stage layout [N0][LDP]
+  static constexpr int LDG = N1 + 1;  // output-row layout [ZR][LDG] (same buffer)
+  static constexpr int PBUF = (N0 * LDP > ZR * LDG) ? N0 * LDP : ZR * LDG;
   static constexpr int TBUF_R = team_buf_stride<N1>();
   static constexpr int TBUF_Z = team_buf_stride<M0>();
   static constexpr int XBUF = (NTEAMS_R * TBUF_R > NTEAMS_Z * TBUF_Z) ? NTEAMS_R * TBUF_R : NTEAMS_Z * TBUF_Z;
   // plane + exchange buffers + tables (rows: N1, z: M0, parity twiddle: N1)
-  static constexpr int SMEM_F2 = N0 * LD + XBUF + N1 + M0 + N1;
+  static constexpr int SMEM_F2 = PBUF + XBUF + N1 + M0 + N1;
+  static_assert(N1 % Q == 0 && N0 % (2 * Q) == 0, "plane split must divide the plane");
+  static_assert(THREADS % 32 == 0 && THREADS % SR == 0 && THREADS % SZ == 0, "teams must tile the CTA");
 };
 
 // Table layout inside one device buffer (float2 entries):
@@ -97,6 +121,7 @@ struct PassArgs {
   int accumulate;               // 1: out += result, 0: out = result
   float lambda;                 // adds lambda * x
   double* dot_partials;         // [nsys][nblocks_c] Re<x, out> partials (nullable)
+  int prefetch_ahead;           // plane pass: L2-prefetch distance in clusters (0 = off)
 };
 
 // ------------------------------------------------------------------------ pass A ----
@@ -153,26 +178,28 @@ expand_fwd_x_kernel(PassArgs a) {
 }
 
 // ------------------------------------------------------------------------ pass B ----
-template <int N0, int N1>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PlaneCfg<N0, N1>::THREADS)
+template <int N0, int N1, int Q, int THREADS_>
+__global__ void __cluster_dims__(2 * Q, 1, 1) __launch_bounds__(THREADS_)
 plane_yz_kernel(PassArgs a) {
   namespace cg = cooperative_groups;
-  using C = PlaneCfg<N0, N1>;
-  constexpr int M0 = C::M0, LD = C::LD;
-  constexpr int SR = C::SR, ER = C::ER, SZ = C::SZ, EZ = C::EZ;
+  using C = PlaneCfg<N0, N1, Q, THREADS_>;
+  constexpr int M0 = C::M0, H = C::H, ZR = C::ZR, LDP = C::LDP, LDG = C::LDG;
+  constexpr int SR = C::SR, ER = C::ER, SZ = C::SZ, EZ = C::EZ, LPT = C::LPT_R;
   extern __shared__ float2 smem[];
-  float2* blk = smem;                 // [N0][LD]
-  float2* xbuf = blk + N0 * LD;
+  float2* P = smem;                   // [N0][LDP] columns, later [ZR][LDG] output rows
+  float2* xbuf = P + C::PBUF;
   float2* tw_r = xbuf + C::XBUF;      // [N1]
   float2* tw_z = tw_r + N1;           // [M0]
   float2* par = tw_z + M0;            // [N1]
 
   cg::cluster_group cluster = cg::this_cluster();
-  const int h = (int)cluster.block_rank();  // ky parity handled by this CTA
+  const int rank = (int)cluster.block_rank();
+  const int h = rank / Q;  // ky parity
+  const int q = rank % Q;  // owned column / row block
   const int slot = blockIdx.y;
   const int kx = blockIdx.z;
   const int sys = slot / a.ncoil;
-  if (a.active && !a.active[sys]) return;  // uniform for both CTAs of the cluster
+  if (a.active && !a.active[sys]) return;  // uniform for the whole cluster
   const int M2 = 2 * a.N2;
 
   const TableOffsets to = table_offsets(N0, N1, a.N2);
@@ -185,92 +212,169 @@ plane_yz_kernel(PassArgs a) {
 
   float2* g = a.spill + ((long long)slot * M2 + kx) * N0 * N1;
   const float* T = a.diag + ((((long long)(a.diag_of_sys ? a.diag_of_sys[sys] : 0) * M2 + kx) * 2 + h) * N1) * M0;
+  float2* Pr[Q];  // column blocks of this parity, one per cluster rank h*Q + q'
+#pragma unroll
+  for (int qq = 0; qq < Q; ++qq) Pr[qq] = cluster.map_shared_rank(P, h * Q + qq);
 
-  // stage 1: rows, forward N1-point FFT of the parity-h half
+  if constexpr (Q == 1) {
+    // the whole plane lands in the (row-major, padded) column buffer in one burst
+    for (int i = threadIdx.x; i < N0 * N1; i += C::THREADS) cp_async8(&P[(i / N1) * LDP + (i % N1)], g + i);
+    cp_async_commit();
+  }
+  {
+    // warm L2 with the plane the cluster one wave ahead will read (PREFETCH_AHEAD
+    // clusters later in launch order); a hint only
+    const long long cl = (long long)blockIdx.z * gridDim.y + blockIdx.y + a.prefetch_ahead;
+    if (a.prefetch_ahead > 0 && cl < (long long)gridDim.y * gridDim.z) {
+      const long long s2 = cl % gridDim.y, k2 = cl / gridDim.y;
+      const char* nxt = (const char*)(a.spill + (s2 * M2 + k2) * N0 * N1);
+      const int bytes = N0 * N1 * (int)sizeof(float2);
+      const int per_cta = bytes / (2 * Q);
+      for (int off = threadIdx.x * 128; off < per_cta; off += C::THREADS * 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt + rank * per_cta + off));
+    }
+  }
+  if constexpr (Q == 1) {
+    cp_async_wait<0>();
+    __syncthreads();
+  }
+
+  // stage 1: owned rows, forward N1-point FFT of the parity-h half; each output column
+  // goes to the CTA that owns it
   {
     const int team = threadIdx.x / SR, t = threadIdx.x % SR;
+    const int tr = row_of_team<SR, C::NTEAMS_R, ZR>(team);
     float2* buf = xbuf + team * C::TBUF_R;
 #pragma unroll 1
-    for (int z0 = 0; z0 < N0; z0 += C::NTEAMS_R) {
-      const int z = z0 + team;
-      const bool ok = z < N0;
+    for (int it = 0; it < LPT; ++it) {
+      const int zl = tr + it * C::NTEAMS_R;
+      const int z = q * ZR + (zl < ZR ? zl : 0);
       float2 v[ER];
 #pragma unroll
       for (int e = 0; e < ER; ++e) {
         const int y = din_index<N1>(t, e);
-        float2 val = ok ? g[(long long)z * N1 + y] : make_float2(0.f, 0.f);
+        float2 val = Q == 1 ? P[z * LDP + y] : g[(long long)z * N1 + y];
         if (h) val = cmul(val, par[y]);
         v[e] = val;
       }
       team_fft_din_to_dout<N1, -1, false>(v, t, buf, tw_r);
-      if (ok) {
+      if (zl < ZR) {
 #pragma unroll
-        for (int r = 0; r < ER; ++r) blk[z * LD + dout_index<N1>(t, r)] = v[r];
-      }
-    }
-  }
-  __syncthreads();
-
-  // stage 2: columns, M0-point FFT along z (upper half zero), x T, inverse, crop
-  {
-    const int team = threadIdx.x / SZ, t = threadIdx.x % SZ;
-    float2* buf = xbuf + team * C::TBUF_Z;
-#pragma unroll 1
-    for (int c0 = 0; c0 < N1; c0 += C::NTEAMS_Z) {
-      const int ky = c0 + team;
-      const bool ok = ky < N1;
-      const int kyc = ok ? ky : 0;
-      float2 v[EZ];
-#pragma unroll
-      for (int e = 0; e < EZ / 2; ++e) v[e] = ok ? blk[din_index<M0>(t, e) * LD + kyc] : make_float2(0.f, 0.f);
-      team_fft_din_to_dout<M0, -1, true>(v, t, buf, tw_z);
-      const float* Tc = T + (long long)kyc * M0;
-#pragma unroll
-      for (int r = 0; r < EZ; ++r) v[r] = cscale(v[r], Tc[dout_index<M0>(t, r)]);
-      team_fft_dout_to_din<M0, 1, true>(v, t, buf, tw_z);
-      if (ok) {
-#pragma unroll
-        for (int e = 0; e < EZ / 2; ++e) blk[din_index<M0>(t, e) * LD + ky] = v[e];
-      }
-    }
-  }
-  __syncthreads();
-
-  // stage 3: rows, inverse N1-point FFT, post-twiddle
-  {
-    const int team = threadIdx.x / SR, t = threadIdx.x % SR;
-    float2* buf = xbuf + team * C::TBUF_R;
-#pragma unroll 1
-    for (int z0 = 0; z0 < N0; z0 += C::NTEAMS_R) {
-      const int z = z0 + team;
-      const bool ok = z < N0;
-      const int zc = ok ? z : 0;
-      float2 v[ER];
-#pragma unroll
-      for (int r = 0; r < ER; ++r) v[r] = blk[zc * LD + dout_index<N1>(t, r)];
-      team_fft_dout_to_din<N1, 1, false>(v, t, buf, tw_r);
-      if (ok) {
-#pragma unroll
-        for (int e = 0; e < ER; ++e) {
-          const int y = din_index<N1>(t, e);
-          blk[z * LD + y] = h ? cmulc(v[e], par[y]) : v[e];
+        for (int r = 0; r < ER; ++r) {
+          const int ky = dout_index<N1>(t, r);
+          Pr[ky / H][z * LDP + ky % H] = v[r];
         }
       }
     }
   }
-  // both halves complete (and all global reads of the plane done) in both CTAs
   cluster.sync();
 
-  // stage 4: sum the two halves, CTA h writes rows [h*N0/2, (h+1)*N0/2)
+  // stage 2: owned columns, M0-point FFT along z (upper half zero), x T, inverse, crop
   {
-    const float2* other = cluster.map_shared_rank(blk, h ^ 1);
-    constexpr int HALF = N0 / 2;
-    for (int i = threadIdx.x; i < HALF * N1; i += C::THREADS) {
-      const int z = h * HALF + i / N1, y = i % N1;
-      g[(long long)z * N1 + y] = cadd(blk[z * LD + y], other[z * LD + y]);
+    const int team = threadIdx.x / SZ, t = threadIdx.x % SZ;
+    float2* buf = xbuf + team * C::TBUF_Z;
+    float2 twz[EZ];  // this lane's z twiddles, reused by every column
+    load_lane_twiddles<M0>(twz, tw_z, t);
+    // the diagonal's columns are fetched one iteration ahead of their use
+    float tnext[EZ];
+    {
+      const int col = team < H ? team : 0;
+      const float* Tc = T + (long long)(q * H + col) * M0;
+#pragma unroll
+      for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tc + dout_index<M0>(t, r));
+    }
+#pragma unroll 1
+    for (int c0 = 0; c0 < H; c0 += C::NTEAMS_Z) {
+      const int col = c0 + team;
+      const bool ok = col < H;
+      const int colc = ok ? col : 0;
+      float tv[EZ];
+#pragma unroll
+      for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
+      if (c0 + C::NTEAMS_Z < H) {
+        const int cn = c0 + C::NTEAMS_Z + team;
+        const float* Tn = T + (long long)(q * H + (cn < H ? cn : 0)) * M0;
+#pragma unroll
+        for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tn + dout_index<M0>(t, r));
+      }
+      float2 v[EZ];
+#pragma unroll
+      for (int e = 0; e < EZ / 2; ++e) v[e] = P[din_index<M0>(t, e) * LDP + colc];
+      team_fft_din_to_dout_r<M0, -1, true>(v, t, buf, twz);
+#pragma unroll
+      for (int r = 0; r < EZ; ++r) v[r] = cscale(v[r], tv[r]);
+      team_fft_dout_to_din_r<M0, 1, true>(v, t, buf, twz);
+      if (ok) {
+#pragma unroll
+        for (int e = 0; e < EZ / 2; ++e) P[din_index<M0>(t, e) * LDP + col] = v[e];
+      }
     }
   }
-  // keep this CTA's shared memory alive until the partner has read it
+  cluster.sync();
+
+  // stage 3: owned rows gathered from the column owners, inverse N1-point FFT along y,
+  // post-twiddle; the result rows overwrite this CTA's buffer once every CTA has read
+  {
+    const int team = threadIdx.x / SR, t = threadIdx.x % SR;
+    const int tr = row_of_team<SR, C::NTEAMS_R, ZR>(team);
+    float2* buf = xbuf + team * C::TBUF_R;
+    if constexpr (Q == 1) {
+      // the row layout is the column layout: each team transforms its rows in place
+#pragma unroll 1
+      for (int it = 0; it < LPT; ++it) {
+        const int zl = tr + it * C::NTEAMS_R;
+        const int zc = zl < ZR ? zl : 0;
+        float2 v[ER];
+#pragma unroll
+        for (int r = 0; r < ER; ++r) v[r] = P[zc * LDP + dout_index<N1>(t, r)];
+        team_fft_dout_to_din<N1, 1, false>(v, t, buf, tw_r);
+        if (zl < ZR) {
+#pragma unroll
+          for (int e = 0; e < ER; ++e) {
+            const int y = din_index<N1>(t, e);
+            P[zl * LDG + y] = h ? cmulc(v[e], par[y]) : v[e];
+          }
+        }
+      }
+    } else {
+      float2 v[LPT][ER];
+#pragma unroll
+      for (int it = 0; it < LPT; ++it) {
+        const int zl = tr + it * C::NTEAMS_R;
+        const int z = q * ZR + (zl < ZR ? zl : 0);
+#pragma unroll
+        for (int r = 0; r < ER; ++r) {
+          const int ky = dout_index<N1>(t, r);
+          v[it][r] = Pr[ky / H][z * LDP + ky % H];
+        }
+      }
+      cluster.sync();  // all column blocks consumed
+#pragma unroll
+      for (int it = 0; it < LPT; ++it) {
+        const int zl = tr + it * C::NTEAMS_R;
+        team_fft_dout_to_din<N1, 1, false>(v[it], t, buf, tw_r);
+        if (zl < ZR) {
+#pragma unroll
+          for (int e = 0; e < ER; ++e) {
+            const int y = din_index<N1>(t, e);
+            P[zl * LDG + y] = h ? cmulc(v[it][e], par[y]) : v[it][e];
+          }
+        }
+      }
+    }
+  }
+  cluster.sync();
+
+  // stage 4: sum the two parities; CTA (h, q) writes the h-th half of rows block q
+  {
+    const float2* other = cluster.map_shared_rank(P, (1 - h) * Q + q);
+    constexpr int HALF = ZR / 2;
+    for (int i = threadIdx.x; i < HALF * N1; i += C::THREADS) {
+      const int zl = h * HALF + i / N1, y = i % N1;
+      g[(long long)(q * ZR + zl) * N1 + y] = cadd(P[zl * LDG + y], other[zl * LDG + y]);
+    }
+  }
+  // keep this CTA's shared memory alive until the partners have read it
   cluster.sync();
 }
 
@@ -281,8 +385,8 @@ inv_x_combine_kernel(PassArgs a) {
   using C = XPassCfg<N2, YT>;
   constexpr int M2 = C::M2, E = C::E, S = C::S, LPT = C::LPT;
   extern __shared__ float2 smem[];
-  float2* tile = smem;
-  float2* xbuf = tile + M2 * C::TILE_LD;
+  float2* tiles = smem;                          // 2 x [M2][TILE_LD]
+  float2* xbuf = tiles + 2 * M2 * C::TILE_LD;
   float2* tw = xbuf + C::NTEAMS * C::TBUF;
   __shared__ double red[32];
 
@@ -297,6 +401,18 @@ inv_x_combine_kernel(PassArgs a) {
   const int team = threadIdx.x / S, t = threadIdx.x % S;
   float2* buf = xbuf + team * C::TBUF;
   const long long plane = (long long)N1 * N2;
+  const long long slot_stride = (long long)M2 * N0 * N1;
+
+  // asynchronous copy of coil ci's [kx][y] tile into tiles[ci & 1]
+  auto prefetch = [&](int ci) {
+    const float2* src = a.spill + (long long)(sys * a.ncoil + ci) * slot_stride + (long long)z * N1 + y0;
+    float2* dst = tiles + (ci & 1) * M2 * C::TILE_LD;
+    for (int i = threadIdx.x; i < M2 * YT; i += C::THREADS) {
+      const int kx = i / YT, j = i % YT;
+      cp_async8(&dst[kx * C::TILE_LD + j], src + (long long)kx * N0 * N1 + j);
+    }
+    cp_async_commit();
+  };
 
   float2 acc[LPT][E / 2];
 #pragma unroll
@@ -304,35 +420,41 @@ inv_x_combine_kernel(PassArgs a) {
 #pragma unroll
     for (int e = 0; e < E / 2; ++e) acc[l][e] = make_float2(0.f, 0.f);
 
+  prefetch(0);
 #pragma unroll 1
   for (int ci = 0; ci < a.ncoil; ++ci) {
-    const int slot = sys * a.ncoil + ci;
-    const int coil = a.coils ? a.coils[ci] : 0;
-    __syncthreads();  // previous coil's tile fully consumed (and the table loaded)
-    const float2* src = a.spill + (long long)slot * M2 * N0 * N1 + (long long)z * N1 + y0;
-    for (int i = threadIdx.x; i < M2 * YT; i += C::THREADS) {
-      const int kx = i / YT, j = i % YT;
-      tile[kx * C::TILE_LD + j] = src[(long long)kx * N0 * N1 + j];
+    if (ci + 1 < a.ncoil) {
+      prefetch(ci + 1);
+      cp_async_wait<1>();  // coil ci's tile has landed
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const int coil = a.coils ? a.coils[ci] : 0;
     const float2* ss = a.smaps ? a.smaps + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
+    const float2* tile = tiles + (ci & 1) * M2 * C::TILE_LD;
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
       const int line = team + l * C::NTEAMS;
+      const long long row = (long long)(y0 + line) * N2;
+      // coil-map (or multiplier) values first: their latency hides behind the FFT
+      float2 m[E / 2];
+#pragma unroll
+      for (int e = 0; e < E / 2; ++e) {
+        const int xi = din_index<M2>(t, e);
+        m[e] = ss ? ss[row + xi] : (a.mul ? a.mul[(long long)z * plane + row + xi] : make_float2(1.f, 0.f));
+      }
       float2 v[E];
 #pragma unroll
       for (int r = 0; r < E; ++r) v[r] = tile[dout_index<M2>(t, r) * C::TILE_LD + line];
       team_fft_dout_to_din<M2, 1, true>(v, t, buf, tw);
-      const long long row = (long long)(y0 + line) * N2;
 #pragma unroll
       for (int e = 0; e < E / 2; ++e) {
-        const int xi = din_index<M2>(t, e);
-        float2 val = v[e];
-        if (ss) val = cmulc(val, ss[row + xi]);
-        else if (a.mul) val = cmul(val, a.mul[(long long)z * plane + row + xi]);
+        const float2 val = ss ? cmulc(v[e], m[e]) : cmul(v[e], m[e]);
         acc[l][e] = cadd(acc[l][e], val);
       }
     }
+    __syncthreads();  // this tile buffer is refilled two coils later
   }
 
   // epilogue
