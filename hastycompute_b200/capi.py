@@ -18,6 +18,8 @@ HB_ERR_CUDA = 3
 HB_ERR_WORKSPACE = 4
 HB_ERR_NOT_PD = 5
 
+HB_NOALLOC_SCRATCH_BYTES = 16 << 20
+
 HB_CG_RUNNING = 0
 HB_CG_CONVERGED = 1
 HB_CG_NOT_PD = 2
@@ -50,6 +52,8 @@ SIGNATURES = {
     "hb_cg_workspace_bytes": (c_size, [c_void_p, c_i64, c_i64, c_int]),
     "hb_cg_run": (c_int, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, P_i64,
                           c_float, c_int, c_double, P_i32, P_i32, c_void_p, c_size, c_void_p]),
+    "hb_toeplitz_apply_noalloc": (c_int, [c_i64, c_i64, c_i64, c_void_p, c_void_p, c_i64, c_i64, c_void_p, c_int,
+                                          c_void_p, c_void_p]),
     "hb_launch_count": (ctypes.c_uint64, []),
     "hb_profile_start": (c_int, []),
     "hb_profile_stop": (c_int, [ctypes.POINTER(c_double), P_i64, c_int]),

@@ -298,6 +298,51 @@ int upload_indices(const int64_t* coils, int64_t ncoil, const int64_t* diag_inde
   return HB_OK;
 }
 
+// Twiddle tables (table_offsets layout), computed in FP64 on the host and rounded.
+void fill_tables(float2* h, int N0, int N1, int N2) {
+  const TableOffsets to = table_offsets(N0, N1, N2);
+  auto team_table = [&](int off, int L) {
+    int E = 0, S = 0;
+    switch (L) {
+      case 8: E = 4; S = 2; break;
+      case 16: E = 4; S = 4; break;
+      case 32: E = 8; S = 4; break;
+      case 64: E = 8; S = 8; break;
+      case 128: E = 16; S = 8; break;
+      case 256: E = 16; S = 16; break;
+    }
+    for (int k1 = 0; k1 < E; ++k1)
+      for (int t = 0; t < S; ++t) {
+        const double a = -2.0 * M_PI * (double)(t * k1) / (double)L;
+        h[off + k1 * S + t] = make_float2((float)std::cos(a), (float)std::sin(a));
+      }
+  };
+  team_table(to.x, 2 * N2);
+  team_table(to.row, N1);
+  team_table(to.z, 2 * N0);
+  for (int y = 0; y < N1; ++y) {
+    const double a = -2.0 * M_PI * (double)y / (double)(2 * N1);
+    h[to.par + y] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+}
+
+// ------------------------------------------------ allocation-free Toeplitz apply ----
+// The spill and the twiddle tables of hb_toeplitz_apply_noalloc live in these arrays;
+// host code reaches them only through cudaGetSymbolAddress (per device).
+constexpr int kNoAllocMaxTables = 2 * 128 + 128 + 2 * 128 + 128;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[HB_NOALLOC_SCRATCH_BYTES];
+static __device__ __align__(256) float2 g_noalloc_tables[kNoAllocMaxTables];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocDevice {
+  bool ready = false;
+  void* scratch = nullptr;
+  float2* tables = nullptr;
+  int dims[3] = {0, 0, 0};  // size the device's tables currently hold
+};
+NoAllocDevice g_noalloc[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
 }  // namespace
 
 extern "C" {
@@ -326,29 +371,7 @@ int hb_plan_create(hb_plan** out, int64_t nz, int64_t ny, int64_t nx, int device
   p->to = table_offsets(p->N0, p->N1, p->N2);
   // twiddle tables in FP64 on the host, rounded to float
   std::vector<float2> h(p->to.total);
-  auto team_table = [&](int off, int L) {
-    int E = 0, S = 0;
-    switch (L) {
-      case 8: E = 4; S = 2; break;
-      case 16: E = 4; S = 4; break;
-      case 32: E = 8; S = 4; break;
-      case 64: E = 8; S = 8; break;
-      case 128: E = 16; S = 8; break;
-      case 256: E = 16; S = 16; break;
-    }
-    for (int k1 = 0; k1 < E; ++k1)
-      for (int t = 0; t < S; ++t) {
-        const double a = -2.0 * M_PI * (double)(t * k1) / (double)L;
-        h[off + k1 * S + t] = make_float2((float)std::cos(a), (float)std::sin(a));
-      }
-  };
-  team_table(p->to.x, 2 * p->N2);
-  team_table(p->to.row, p->N1);
-  team_table(p->to.z, 2 * p->N0);
-  for (int y = 0; y < p->N1; ++y) {
-    const double a = -2.0 * M_PI * (double)y / (double)(2 * p->N1);
-    h[p->to.par + y] = make_float2((float)std::cos(a), (float)std::sin(a));
-  }
+  fill_tables(h.data(), p->N0, p->N1, p->N2);
   cudaError_t e = cudaMalloc(&p->tables, h.size() * sizeof(float2));
   if (e == cudaSuccess) e = cudaMemcpy(p->tables, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -637,6 +660,67 @@ int hb_cg_run(const hb_plan* p, int64_t nsys, void* x, const void* b, const void
   }
   if (notpd) return fail(HB_ERR_NOT_PD, "A was not positive definite");
   return HB_OK;
+}
+
+int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in, void* out, int64_t out_ldz,
+                              int64_t out_ldy, const void* mul, int accumulate, const float* packed_diag,
+                              void* stream) {
+  if (!hb_size_supported(nz, ny, nx))
+    return fail(HB_ERR_UNSUPPORTED, "hb_toeplitz_apply_noalloc: image size not supported");
+  if (!in || !out || !packed_diag) return fail(HB_ERR_INVALID, "hb_toeplitz_apply_noalloc: NULL pointer");
+  const unsigned long long need = 16ull * (unsigned long long)(nz * ny * nx);
+  if (need > HB_NOALLOC_SCRATCH_BYTES)
+    return fail(HB_ERR_WORKSPACE, "hb_toeplitz_apply_noalloc: " + std::to_string(nz) + "x" + std::to_string(ny) + "x" +
+                                      std::to_string(nx) + " needs " + std::to_string(need) +
+                                      " bytes of scratch, more than the built-in " +
+                                      std::to_string((unsigned long long)HB_NOALLOC_SCRATCH_BYTES) +
+                                      " (use hb_toeplitz_apply with a caller workspace)");
+  int dev = 0;
+  HB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(HB_ERR_INVALID, "hb_toeplitz_apply_noalloc: device index");
+  cudaStream_t st = (cudaStream_t)stream;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  NoAllocDevice& d = g_noalloc[dev];
+  if (!d.ready) {  // once per device, with that device current
+    HB_CUDA(cudaGetSymbolAddress(&d.scratch, g_noalloc_scratch));
+    HB_CUDA(cudaGetSymbolAddress((void**)&d.tables, g_noalloc_tables));
+    d.ready = true;
+  }
+  if (d.dims[0] != nz || d.dims[1] != ny || d.dims[2] != nx) {
+    float2 h[kNoAllocMaxTables];  // host stack, no heap
+    fill_tables(h, (int)nz, (int)ny, (int)nx);
+    const int n = table_offsets((int)nz, (int)ny, (int)nx).total;
+    HB_CUDA(cudaMemcpyAsync(d.tables, h, n * sizeof(float2), cudaMemcpyHostToDevice, st));
+    HB_CUDA(cudaStreamSynchronize(st));  // the host array leaves scope
+    d.dims[0] = (int)nz;
+    d.dims[1] = (int)ny;
+    d.dims[2] = (int)nx;
+  }
+  hb_plan p;
+  p.N0 = (int)nz;
+  p.N1 = (int)ny;
+  p.N2 = (int)nx;
+  p.device = dev;
+  p.tables = d.tables;
+  p.to = table_offsets(p.N0, p.N1, p.N2);
+  PassArgs a{};
+  a.N0 = p.N0; a.N1 = p.N1; a.N2 = p.N2;
+  a.nsys = 1; a.ncoil = 1;
+  a.coils = nullptr; a.diag_of_sys = nullptr; a.active = nullptr;
+  a.x = (const float2*)in;
+  a.smaps = nullptr;
+  a.mul = (const float2*)mul;
+  a.spill = (float2*)d.scratch;
+  a.diag = packed_diag;
+  a.tables = d.tables;
+  a.out = (float2*)out;
+  a.out_sys_stride = 0;
+  a.out_ldz = out_ldz;
+  a.out_ldy = out_ldy;
+  a.accumulate = accumulate ? 1 : 0;
+  a.lambda = 0.f;
+  a.dot_partials = nullptr;
+  return run_normal(&p, a, st);
 }
 
 uint64_t hb_launch_count(void) { return g_launches.load(); }

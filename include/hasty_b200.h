@@ -124,6 +124,31 @@ int hb_cg_run(const hb_plan* plan, int64_t nsys, void* x, const void* b, const v
               int32_t* status_host, int32_t* iters_done_host, void* workspace,
               size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of hb_toeplitz_apply.  No counterpart in the reference.
+ *
+ * For callers that may not allocate device memory themselves, e.g. reconstruction
+ * plugins that run inside a host application that owns a fixed device-memory budget,
+ * or code under a memory manager that forbids cudaMalloc after start-up.  It needs no
+ * plan and no workspace: the scratch (the 2 * nz * ny * nx complex64 spill of the
+ * three passes) is a file-scope device array of HB_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading this library holds until the process exits, and the twiddle tables live in a
+ * second small device array.  The caller still passes the input, the output and the
+ * packed diagonal (hb_diag_pack / hb_diag_build write into caller memory).
+ *
+ * Limits and behaviour:
+ *  - 16 * nz * ny * nx must not exceed HB_NOALLOC_SCRATCH_BYTES (16 MiB: up to 2^20
+ *    voxels, e.g. 128 x 128 x 64); larger sizes return HB_ERR_WORKSPACE with a message.
+ *  - Works on the calling thread's current device.  The first call on a device looks up
+ *    the arrays' device addresses; make that first call before any stream capture.
+ *  - All calls share the arrays, which keep the last call's contents (nothing in them
+ *    needs to start at zero).  Calls that overlap on the GPU (several streams or
+ *    threads) race on the shared scratch: serialise them.
+ *  - Calls no cudaMalloc, cudaFree or other allocating routine. */
+#define HB_NOALLOC_SCRATCH_BYTES (16u << 20)
+int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in, void* out,
+                              int64_t out_ldz, int64_t out_ldy, const void* mul, int accumulate,
+                              const float* packed_diag, void* stream);
+
 /* ---- measurement hooks (no counterpart in the reference; used by benchmarks) ----
  * Kernel kinds for the profile counters. */
 #define HB_KERNEL_EXPAND_FWD_X 0   /* pass A */
