@@ -47,7 +47,20 @@ int fail(int code, const std::string& msg) {
       return fail(HB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(_e)); \
   } while (0)
 
-bool pow2_in_range(int64_t n) { return n >= 8 && n <= 128 && (n & (n - 1)) == 0; }
+// Supported axis lengths and their row in the launcher tables.
+int axis_index(int64_t n) {
+  switch (n) {
+    case 8: return 0;
+    case 16: return 1;
+    case 32: return 2;
+    case 64: return 3;
+    case 128: return 4;
+    case 96: return 5;
+    case 160: return 6;
+    default: return -1;
+  }
+}
+bool is_pow2_axis(int64_t n) { int i = axis_index(n); return i >= 0 && i <= 4; }
 int ilog2(int n) {
   int l = 0;
   while ((1 << l) < n) ++l;
@@ -205,10 +218,12 @@ int plane_variant_index(int nvariants) {
 
 // [log2(N2)-3][log2(YT)-3]
 #define HB_XROW(N2, F) {&F<N2, 8>, &F<N2, 16>}
-const PassLauncher kLaunchA[5][2] = {HB_XROW(8, launch_a), HB_XROW(16, launch_a), HB_XROW(32, launch_a),
-                                     HB_XROW(64, launch_a), HB_XROW(128, launch_a)};
-const PassLauncher kLaunchC[5][2] = {HB_XROW(8, launch_c), HB_XROW(16, launch_c), HB_XROW(32, launch_c),
-                                     HB_XROW(64, launch_c), HB_XROW(128, launch_c)};
+const PassLauncher kLaunchA[7][2] = {HB_XROW(8, launch_a),   HB_XROW(16, launch_a), HB_XROW(32, launch_a),
+                                     HB_XROW(64, launch_a),  HB_XROW(128, launch_a), HB_XROW(96, launch_a),
+                                     HB_XROW(160, launch_a)};
+const PassLauncher kLaunchC[7][2] = {HB_XROW(8, launch_c),   HB_XROW(16, launch_c), HB_XROW(32, launch_c),
+                                     HB_XROW(64, launch_c),  HB_XROW(128, launch_c), HB_XROW(96, launch_c),
+                                     HB_XROW(160, launch_c)};
 #define HB_BROW(N0)                                                                                    \
   {&launch_b<N0, 8, 1, 128>, &launch_b<N0, 16, 1, 128>, &launch_b<N0, 32, 1, 128>, &launch_b<N0, 64, 1, 256>, \
    &launch_b<N0, 128, 1, 512>}
@@ -217,6 +232,8 @@ const PassLauncher kLaunchB[5][5] = {HB_BROW(8), HB_BROW(16), HB_BROW(32), HB_BR
 PassLauncher plane_launcher(int N0, int N1) {
   if (N0 == 128 && N1 == 128) return kPlane128[plane_variant_index(5)].fn;
   if (N0 == 64 && N1 == 64) return kPlane64[plane_variant_index(4)].fn;
+  if (N0 == 96 && N1 == 96) return &launch_b<96, 96, 1, 256>;
+  if (N0 == 160 && N1 == 160) return &launch_b<160, 160, 2, 128>;
   return kLaunchB[ilog2(N0) - 3][ilog2(N1) - 3];
 }
 
@@ -225,7 +242,7 @@ int yt_for(int N1) { return N1 < 16 ? N1 : 16; }
 // Runs passes A, B, C for `nsys` systems described by `a`.
 int run_normal(const hb_plan* p, PassArgs a, cudaStream_t st) {
   const int yt = yt_for(p->N1);
-  const int ia = ilog2(p->N2) - 3, iy = ilog2(yt) - 3;
+  const int ia = axis_index(p->N2), iy = ilog2(yt) - 3;
   const int nslots = a.nsys * a.ncoil;
   if (nslots > 65535) return fail(HB_ERR_INVALID, "too many system x coil slots in one launch (max 65535)");
   cudaError_t e = kLaunchA[ia][iy](a, nslots, st);
@@ -310,6 +327,10 @@ void fill_tables(float2* h, int N0, int N1, int N2) {
       case 64: E = 8; S = 8; break;
       case 128: E = 16; S = 8; break;
       case 256: E = 16; S = 16; break;
+      case 96: E = 24; S = 4; break;
+      case 160: E = 40; S = 4; break;
+      case 192: E = 24; S = 8; break;
+      case 320: E = 40; S = 8; break;
     }
     for (int k1 = 0; k1 < E; ++k1)
       for (int t = 0; t < S; ++t) {
@@ -329,7 +350,7 @@ void fill_tables(float2* h, int N0, int N1, int N2) {
 // ------------------------------------------------ allocation-free Toeplitz apply ----
 // The spill and the twiddle tables of hb_toeplitz_apply_noalloc live in these arrays;
 // host code reaches them only through cudaGetSymbolAddress (per device).
-constexpr int kNoAllocMaxTables = 2 * 128 + 128 + 2 * 128 + 128;
+constexpr int kNoAllocMaxTables = 2 * 160 + 160 + 2 * 160 + 160;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[HB_NOALLOC_SCRATCH_BYTES];
 static __device__ __align__(256) float2 g_noalloc_tables[kNoAllocMaxTables];
 
@@ -352,7 +373,9 @@ int hb_version(void) { return 100; }
 const char* hb_last_error(void) { return g_err.c_str(); }
 
 int hb_size_supported(int64_t nz, int64_t ny, int64_t nx) {
-  return pow2_in_range(nz) && pow2_in_range(ny) && pow2_in_range(nx) ? 1 : 0;
+  if (axis_index(nz) < 0 || axis_index(ny) < 0 || axis_index(nx) < 0) return 0;
+  const bool plane_ok = (is_pow2_axis(nz) && is_pow2_axis(ny)) || (nz == 96 && ny == 96) || (nz == 160 && ny == 160);
+  return plane_ok ? 1 : 0;
 }
 
 int hb_plan_create(hb_plan** out, int64_t nz, int64_t ny, int64_t nx, int device) {
@@ -360,7 +383,9 @@ int hb_plan_create(hb_plan** out, int64_t nz, int64_t ny, int64_t nx, int device
   *out = nullptr;
   if (!hb_size_supported(nz, ny, nx))
     return fail(HB_ERR_UNSUPPORTED, "image size " + std::to_string(nz) + "x" + std::to_string(ny) + "x" +
-                                        std::to_string(nx) + " not supported (each axis a power of two in [8, 128])");
+                                        std::to_string(nx) +
+                                        " not supported (axes in {8,16,32,64,128}, or nz = ny in {96, 160}; nx in "
+                                        "{8,16,32,64,96,128,160})");
   DeviceGuard dg(device);
   if (!dg.ok) return fail(HB_ERR_CUDA, "cannot select device " + std::to_string(device));
   hb_plan* p = new hb_plan();

@@ -39,6 +39,41 @@ HB_DEV float2 tw16(float2 a) {
   }
 }
 
+// ---- compile-time cos/sin of 2*pi*p/R for any R (Taylor series, evaluated by the compiler) ----
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double ct_sin_series(double x) {
+  double term = x, sum = x;
+  for (int k = 1; k < 30; ++k) {
+    term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+    sum += term;
+  }
+  return sum;
+}
+// reduce to [-pi, pi] first so the series converges fast
+constexpr double ct_reduce(double x) {
+  while (x > 0.5 * kTwoPi) x -= kTwoPi;
+  while (x < -0.5 * kTwoPi) x += kTwoPi;
+  return x;
+}
+constexpr double ct_sin(double x) { return ct_sin_series(ct_reduce(x)); }
+constexpr double ct_cos(double x) { return ct_sin_series(ct_reduce(x + 0.25 * kTwoPi)); }
+
+// multiply by exp(DIR * 2*pi*i * P / R)
+template <int R, int P, int DIR>
+HB_DEV float2 twR(float2 a) {
+  constexpr int p = ((P % R) + R) % R;
+  if constexpr (p == 0) return a;
+  else if constexpr (4 * p == R) return rot90<DIR>(a);
+  else if constexpr (2 * p == R) return make_float2(-a.x, -a.y);
+  else if constexpr (4 * p == 3 * R) return rot90<-DIR>(a);
+  else {
+    constexpr float c = (float)ct_cos(kTwoPi * p / R);
+    constexpr float s0 = (float)ct_sin(kTwoPi * p / R);
+    constexpr float s = DIR < 0 ? -s0 : s0;
+    return crot(a, c, s);
+  }
+}
+
 template <int DIR>
 HB_DEV void dft2(float2& a, float2& b) {
   float2 t = a;
@@ -111,10 +146,94 @@ struct Dft<16, DIR> {
   }
 };
 
+template <int DIR>
+struct Dft<3, DIR> {
+  // X1,2 = a - (b+c)/2 +- i*DIR*(sqrt(3)/2)*(b - c)
+  static HB_DEV void run(float2* v) {
+    constexpr float h = 0.86602540378443865f;  // sqrt(3)/2
+    const float2 a = v[0], t1 = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+    const float2 m = make_float2(fmaf(-0.5f, t1.x, a.x), fmaf(-0.5f, t1.y, a.y));
+    const float2 r = rot90<DIR>(cscale(d, h));
+    v[0] = cadd(a, t1);
+    v[1] = cadd(m, r);
+    v[2] = csub(m, r);
+  }
+};
+template <int DIR>
+struct Dft<5, DIR> {
+  static HB_DEV void run(float2* v) {
+    constexpr float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;   // cos(2pi/5), cos(4pi/5)
+    constexpr float s1 = 0.95105651629515357f, s2 = 0.58778525229247313f;    // sin(2pi/5), sin(4pi/5)
+    const float2 x0 = v[0];
+    const float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    const float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    const float2 a1 = make_float2(x0.x + c1 * t1.x + c2 * t2.x, x0.y + c1 * t1.y + c2 * t2.y);
+    const float2 a2 = make_float2(x0.x + c2 * t1.x + c1 * t2.x, x0.y + c2 * t1.y + c1 * t2.y);
+    // b1 = s1 t3 + s2 t4, b2 = s2 t3 - s1 t4, multiplied by DIR * i
+    const float2 b1 = rot90<DIR>(make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
+    const float2 b2 = rot90<DIR>(make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
+    v[0] = cadd(x0, cadd(t1, t2));
+    v[1] = cadd(a1, b1);
+    v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2);
+    v[3] = csub(a2, b2);
+  }
+};
+
+// Mixed radix R = R1 * R2:  n = n1 + R1*n2,  k = k2 + R2*k1
+//   R2-point DFTs over n2, twiddle w_R^(n1*k2), R1-point DFTs over n1.
+template <int R1, int R2, int DIR>
+struct DftMixed {
+  static constexpr int R = R1 * R2;
+  template <int N1 = 0, int K2 = 0>
+  static HB_DEV void twiddle(float2 (&y)[R1][R2]) {
+    if constexpr (N1 < R1) {
+      if constexpr (K2 < R2) {
+        y[N1][K2] = twR<R, N1 * K2, DIR>(y[N1][K2]);
+        twiddle<N1, K2 + 1>(y);
+      } else {
+        twiddle<N1 + 1, 0>(y);
+      }
+    }
+  }
+  static HB_DEV void run(float2* v) {
+    float2 y[R1][R2];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) y[n1][n2] = v[n1 + R1 * n2];
+      Dft<R2, DIR>::run(y[n1]);
+    }
+    twiddle(y);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      float2 u[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) u[n1] = y[n1][k2];
+      Dft<R1, DIR>::run(u);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) v[k2 + R2 * k1] = u[k1];
+    }
+  }
+};
+template <int DIR> struct Dft<6, DIR> : DftMixed<3, 2, DIR> {};
+template <int DIR> struct Dft<10, DIR> : DftMixed<5, 2, DIR> {};
+template <int DIR> struct Dft<12, DIR> : DftMixed<3, 4, DIR> {};
+template <int DIR> struct Dft<20, DIR> : DftMixed<5, 4, DIR> {};
+template <int DIR> struct Dft<24, DIR> : DftMixed<3, 8, DIR> {};
+template <int DIR> struct Dft<40, DIR> : DftMixed<5, 8, DIR> {};
+
 // DFT of size R whose inputs v[R/2..R-1] are zero (they are not read).
 // X[2k] = DFT_{R/2}(v)[k];  X[2k+1] = DFT_{R/2}(v[n] * w_R^n)[k]
 template <int R, int DIR>
 struct DftHalfIn {
+  template <int N>
+  static HB_DEV void twiddle_half(const float2* v, float2* b) {
+    if constexpr (N < R / 2) {
+      b[N] = twR<R, N, DIR>(v[N]);
+      twiddle_half<N + 1>(v, b);
+    }
+  }
   static HB_DEV void run(float2* v) {
     constexpr int H = R / 2;
     float2 a[H], b[H];
@@ -131,7 +250,7 @@ struct DftHalfIn {
       b[4] = tw16<4, DIR>(v[4]); b[5] = tw16<5, DIR>(v[5]); b[6] = tw16<6, DIR>(v[6]);
       b[7] = tw16<7, DIR>(v[7]);
     } else {
-      static_assert(R <= 16, "DftHalfIn: size not supported");
+      twiddle_half<1>(v, b);
     }
     Dft<H, DIR>::run(a);
     Dft<H, DIR>::run(b);
@@ -149,6 +268,10 @@ template <> struct TeamCfg<32> { static constexpr int E = 8, S = 4; };
 template <> struct TeamCfg<64> { static constexpr int E = 8, S = 8; };
 template <> struct TeamCfg<128> { static constexpr int E = 16, S = 8; };
 template <> struct TeamCfg<256> { static constexpr int E = 16, S = 16; };
+template <> struct TeamCfg<96> { static constexpr int E = 24, S = 4; };
+template <> struct TeamCfg<160> { static constexpr int E = 40, S = 4; };
+template <> struct TeamCfg<192> { static constexpr int E = 24, S = 8; };
+template <> struct TeamCfg<320> { static constexpr int E = 40, S = 8; };
 
 // Shared-memory float2 slots one team needs for its exchange buffer.  The stride is
 // chosen so that teams sharing a half-warp land on disjoint banks.

@@ -73,15 +73,19 @@ struct PlaneCfg {
   static constexpr int NTEAMS_R = THREADS / SR;
   static constexpr int NTEAMS_Z = THREADS / SZ;
   static constexpr int LPT_R = (ZR + NTEAMS_R - 1) / NTEAMS_R;  // rows per team
-  static constexpr int LDP = H + 1;   // column-stage layout [N0][LDP]
-  static constexpr int LDG = N1 + 1;  // output-row layout [ZR][LDG] (same buffer)
-  static constexpr int PBUF = (N0 * LDP > ZR * LDG) ? N0 * LDP : ZR * LDG;
+  static constexpr int LDP = H + 1;   // column-stage row pitch
+  // Row z of the column stage sits at buffer row pos(z) = Q*(z % ZR) + z / ZR, so the Q
+  // rows that every CTA of the cluster consumes in one round of the inverse row stage
+  // are adjacent; output row zl then overwrites exactly those Q*LDP >= N1 + 1 slots.
+  static constexpr int PBUF = N0 * LDP;
+  static constexpr int GROW = Q * LDP;  // output-row pitch
   static constexpr int TBUF_R = team_buf_stride<N1>();
   static constexpr int TBUF_Z = team_buf_stride<M0>();
   static constexpr int XBUF = (NTEAMS_R * TBUF_R > NTEAMS_Z * TBUF_Z) ? NTEAMS_R * TBUF_R : NTEAMS_Z * TBUF_Z;
   // plane + exchange buffers + tables (rows: N1, z: M0, parity twiddle: N1)
   static constexpr int SMEM_F2 = PBUF + XBUF + N1 + M0 + N1;
   static_assert(N1 % Q == 0 && N0 % (2 * Q) == 0, "plane split must divide the plane");
+  static_assert(GROW >= N1, "an output row must fit in the rows it replaces");
   static_assert(THREADS % 32 == 0 && THREADS % SR == 0 && THREADS % SZ == 0, "teams must tile the CTA");
 };
 
@@ -183,7 +187,8 @@ __global__ void __cluster_dims__(2 * Q, 1, 1) __launch_bounds__(THREADS_)
 plane_yz_kernel(PassArgs a) {
   namespace cg = cooperative_groups;
   using C = PlaneCfg<N0, N1, Q, THREADS_>;
-  constexpr int M0 = C::M0, H = C::H, ZR = C::ZR, LDP = C::LDP, LDG = C::LDG;
+  constexpr int M0 = C::M0, H = C::H, ZR = C::ZR, LDP = C::LDP, GROW = C::GROW;
+  auto pos = [](int z) { return Q * (z % ZR) + z / ZR; };
   constexpr int SR = C::SR, ER = C::ER, SZ = C::SZ, EZ = C::EZ, LPT = C::LPT_R;
   extern __shared__ float2 smem[];
   float2* P = smem;                   // [N0][LDP] columns, later [ZR][LDG] output rows
@@ -262,7 +267,7 @@ plane_yz_kernel(PassArgs a) {
 #pragma unroll
         for (int r = 0; r < ER; ++r) {
           const int ky = dout_index<N1>(t, r);
-          Pr[ky / H][z * LDP + ky % H] = v[r];
+          Pr[ky / H][pos(z) * LDP + ky % H] = v[r];
         }
       }
     }
@@ -273,8 +278,10 @@ plane_yz_kernel(PassArgs a) {
   {
     const int team = threadIdx.x / SZ, t = threadIdx.x % SZ;
     float2* buf = xbuf + team * C::TBUF_Z;
-    float2 twz[EZ];  // this lane's z twiddles, reused by every column
-    load_lane_twiddles<M0>(twz, tw_z, t);
+    // this lane's z twiddles, reused by every column (registers when they are few)
+    constexpr bool kRegTw = EZ <= 16;
+    float2 twz[kRegTw ? EZ : 1];
+    if constexpr (kRegTw) load_lane_twiddles<M0>(twz, tw_z, t);
     // the diagonal's columns are fetched one iteration ahead of their use
     float tnext[EZ];
     {
@@ -299,66 +306,44 @@ plane_yz_kernel(PassArgs a) {
       }
       float2 v[EZ];
 #pragma unroll
-      for (int e = 0; e < EZ / 2; ++e) v[e] = P[din_index<M0>(t, e) * LDP + colc];
-      team_fft_din_to_dout_r<M0, -1, true>(v, t, buf, twz);
+      for (int e = 0; e < EZ / 2; ++e) v[e] = P[pos(din_index<M0>(t, e)) * LDP + colc];
+      if constexpr (kRegTw) team_fft_din_to_dout_r<M0, -1, true>(v, t, buf, twz);
+      else team_fft_din_to_dout<M0, -1, true>(v, t, buf, tw_z);
 #pragma unroll
       for (int r = 0; r < EZ; ++r) v[r] = cscale(v[r], tv[r]);
-      team_fft_dout_to_din_r<M0, 1, true>(v, t, buf, twz);
+      if constexpr (kRegTw) team_fft_dout_to_din_r<M0, 1, true>(v, t, buf, twz);
+      else team_fft_dout_to_din<M0, 1, true>(v, t, buf, tw_z);
       if (ok) {
 #pragma unroll
-        for (int e = 0; e < EZ / 2; ++e) P[din_index<M0>(t, e) * LDP + col] = v[e];
+        for (int e = 0; e < EZ / 2; ++e) P[pos(din_index<M0>(t, e)) * LDP + col] = v[e];
       }
     }
   }
   cluster.sync();
 
   // stage 3: owned rows gathered from the column owners, inverse N1-point FFT along y,
-  // post-twiddle; the result rows overwrite this CTA's buffer once every CTA has read
+  // post-twiddle.  Output row zl replaces the Q buffer rows consumed in the same round.
   {
     const int team = threadIdx.x / SR, t = threadIdx.x % SR;
     const int tr = row_of_team<SR, C::NTEAMS_R, ZR>(team);
     float2* buf = xbuf + team * C::TBUF_R;
-    if constexpr (Q == 1) {
-      // the row layout is the column layout: each team transforms its rows in place
 #pragma unroll 1
-      for (int it = 0; it < LPT; ++it) {
-        const int zl = tr + it * C::NTEAMS_R;
-        const int zc = zl < ZR ? zl : 0;
-        float2 v[ER];
+    for (int it = 0; it < LPT; ++it) {
+      const int zl = tr + it * C::NTEAMS_R;
+      const int z = q * ZR + (zl < ZR ? zl : 0);
+      float2 v[ER];
 #pragma unroll
-        for (int r = 0; r < ER; ++r) v[r] = P[zc * LDP + dout_index<N1>(t, r)];
-        team_fft_dout_to_din<N1, 1, false>(v, t, buf, tw_r);
-        if (zl < ZR) {
-#pragma unroll
-          for (int e = 0; e < ER; ++e) {
-            const int y = din_index<N1>(t, e);
-            P[zl * LDG + y] = h ? cmulc(v[e], par[y]) : v[e];
-          }
-        }
+      for (int r = 0; r < ER; ++r) {
+        const int ky = dout_index<N1>(t, r);
+        v[r] = Pr[ky / H][pos(z) * LDP + ky % H];
       }
-    } else {
-      float2 v[LPT][ER];
+      if constexpr (Q > 1) cluster.sync();  // every CTA has read this round's rows
+      team_fft_dout_to_din<N1, 1, false>(v, t, buf, tw_r);
+      if (zl < ZR) {
 #pragma unroll
-      for (int it = 0; it < LPT; ++it) {
-        const int zl = tr + it * C::NTEAMS_R;
-        const int z = q * ZR + (zl < ZR ? zl : 0);
-#pragma unroll
-        for (int r = 0; r < ER; ++r) {
-          const int ky = dout_index<N1>(t, r);
-          v[it][r] = Pr[ky / H][z * LDP + ky % H];
-        }
-      }
-      cluster.sync();  // all column blocks consumed
-#pragma unroll
-      for (int it = 0; it < LPT; ++it) {
-        const int zl = tr + it * C::NTEAMS_R;
-        team_fft_dout_to_din<N1, 1, false>(v[it], t, buf, tw_r);
-        if (zl < ZR) {
-#pragma unroll
-          for (int e = 0; e < ER; ++e) {
-            const int y = din_index<N1>(t, e);
-            P[zl * LDG + y] = h ? cmulc(v[it][e], par[y]) : v[it][e];
-          }
+        for (int e = 0; e < ER; ++e) {
+          const int y = din_index<N1>(t, e);
+          P[zl * GROW + y] = h ? cmulc(v[e], par[y]) : v[e];
         }
       }
     }
@@ -371,7 +356,7 @@ plane_yz_kernel(PassArgs a) {
     constexpr int HALF = ZR / 2;
     for (int i = threadIdx.x; i < HALF * N1; i += C::THREADS) {
       const int zl = h * HALF + i / N1, y = i % N1;
-      g[(long long)(q * ZR + zl) * N1 + y] = cadd(P[zl * LDG + y], other[zl * LDG + y]);
+      g[(long long)(q * ZR + zl) * N1 + y] = cadd(P[zl * GROW + y], other[zl * GROW + y]);
     }
   }
   // keep this CTA's shared memory alive until the partners have read it

@@ -32,7 +32,10 @@ def test_sizes_and_errors_without_gpu():
     assert lib.hb_version() >= 100
     assert lib.hb_size_supported(128, 128, 128) == 1
     assert lib.hb_size_supported(64, 32, 16) == 1
-    assert lib.hb_size_supported(96, 96, 96) == 0
+    assert lib.hb_size_supported(96, 96, 96) == 1
+    assert lib.hb_size_supported(160, 160, 128) == 1
+    assert lib.hb_size_supported(96, 128, 96) == 0
+    assert lib.hb_size_supported(80, 80, 80) == 0
     assert lib.hb_size_supported(256, 128, 128) == 0
     h = ctypes.c_void_p()
     assert lib.hb_plan_create(ctypes.byref(h), 12, 16, 16, 0) == capi.HB_ERR_UNSUPPORTED

@@ -31,7 +31,8 @@ def _case(shape, ncoil, K, seed):
     return coords, x, sm, T
 
 
-SHAPES = [(8, 8, 8), (8, 16, 32), (32, 8, 16), (16, 16, 16), (32, 32, 32), (64, 32, 16)]
+SHAPES = [(8, 8, 8), (8, 16, 32), (32, 8, 16), (16, 16, 16), (32, 32, 32), (64, 32, 16),
+          (8, 8, 96), (16, 16, 160), (96, 96, 16), (160, 160, 8)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -243,3 +244,18 @@ def test_plane_variants_agree(cuda, shape, nvar, monkeypatch):
         outs.append(out)
     for v in range(1, nvar):
         assert torch.equal(outs[0], outs[v]), v
+
+
+@pytest.mark.parametrize("shape,ncoil", [((96, 96, 96), 3), ((160, 160, 128), 2)])
+def test_sense_normal_non_power_of_two(cuda, shape, ncoil):
+    """The uneven-batch image sizes (radix-3 and radix-5 FFT lengths) against the FP64 oracle."""
+    plan = ToeplitzPlan(shape, cuda)
+    coords = synth.kooshball(128, 2 * shape[0])
+    packed, Tg = plan.build_diagonal(torch.from_numpy(coords), want_complex=True)
+    T = _np(Tg)
+    sm = synth.coil_maps(ncoil, shape, seed=11)
+    x = synth.gaussian_image(shape, seed=12)
+    out = torch.empty(shape, dtype=torch.complex64, device=cuda)
+    plan.sense_normal(_c64(x, cuda), out, _c64(sm, cuda), packed, lam=1e-3)
+    ref = O.sense_normal_toeplitz(x, sm, T) + 1e-3 * x
+    assert O.rel_l2(_np(out), ref) < TOL
