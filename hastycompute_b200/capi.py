@@ -33,6 +33,18 @@ c_double = ctypes.c_double
 P_i64 = ctypes.POINTER(ctypes.c_int64)
 P_i32 = ctypes.POINTER(ctypes.c_int32)
 
+HB_CG_GRAPH = 1
+
+
+class HbSystem(ctypes.Structure):
+    """struct hb_system (include/hasty_b200.h)."""
+    _fields_ = [("x", ctypes.c_void_p), ("out", ctypes.c_void_p), ("b", ctypes.c_void_p),
+                ("smaps", ctypes.c_void_p), ("coils", ctypes.POINTER(ctypes.c_int64)), ("ncoil", ctypes.c_int64),
+                ("packed_diag", ctypes.c_void_p), ("lam", ctypes.c_float)]
+
+
+P_sys = ctypes.POINTER(HbSystem)
+
 # name -> (restype, argtypes); one entry per declaration of include/hasty_b200.h
 SIGNATURES = {
     "hb_version": (c_int, []),
@@ -49,6 +61,10 @@ SIGNATURES = {
                                   c_void_p, c_size, c_void_p]),
     "hb_sense_normal_apply": (c_int, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p,
                                       P_i64, c_float, c_void_p, c_size, c_void_p]),
+    "hb_systems_workspace_bytes": (c_size, [c_void_p, c_i64, c_i64, c_int]),
+    "hb_sense_normal_apply_systems": (c_int, [c_void_p, c_i64, P_sys, c_void_p, c_size, c_void_p]),
+    "hb_cg_run_systems": (c_int, [c_void_p, c_i64, P_sys, c_int, c_double, c_int, P_i32, P_i32, c_void_p, c_size,
+                                  c_void_p]),
     "hb_cg_workspace_bytes": (c_size, [c_void_p, c_i64, c_i64, c_int]),
     "hb_cg_run": (c_int, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, P_i64,
                           c_float, c_int, c_double, P_i32, P_i32, c_void_p, c_size, c_void_p]),

@@ -109,6 +109,8 @@ struct LaunchScope {
   cudaStream_t st;
   cudaEvent_t a = nullptr, b = nullptr;
   LaunchScope(int k, cudaStream_t s) : kind(k), st(s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;  // graph replays count
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (g_prof_on.load(std::memory_order_relaxed)) {
       a = take_event();
@@ -139,10 +141,20 @@ struct Arena {
   }
 };
 
-template <typename K>
-cudaError_t ensure_smem(K kernel, size_t bytes) {
+// Opt-in to large dynamic shared memory, once per kernel and device (the first call of
+// a kernel on a device happens outside any stream capture).
+template <auto kernel>
+cudaError_t ensure_smem(size_t bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  static std::atomic<uint64_t> done{0};  // one flag set per kernel, one bit per device
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (done.load() & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done.fetch_or(bit);
+  return e;
 }
 
 // ---------------------------------------------------------------- pass launchers ----
@@ -152,7 +164,7 @@ template <int N2, int YT>
 cudaError_t launch_a(const PassArgs& a, int nslots, cudaStream_t st) {
   using C = XPassCfg<N2, YT>;
   const size_t smem = C::SMEM_F2 * sizeof(float2);
-  cudaError_t e = ensure_smem(expand_fwd_x_kernel<N2, YT>, smem);
+  cudaError_t e = ensure_smem<expand_fwd_x_kernel<N2, YT>>(smem);
   if (e != cudaSuccess) return e;
   dim3 grid(a.N1 / YT, a.N0, nslots);
   LaunchScope ls(HB_KERNEL_EXPAND_FWD_X, st);
@@ -164,7 +176,7 @@ template <int N2, int YT>
 cudaError_t launch_c(const PassArgs& a, int nsys, cudaStream_t st) {
   using C = XPassCfg<N2, YT>;
   const size_t smem = C::SMEM_F2_C * sizeof(float2);
-  cudaError_t e = ensure_smem(inv_x_combine_kernel<N2, YT>, smem);
+  cudaError_t e = ensure_smem<inv_x_combine_kernel<N2, YT>>(smem);
   if (e != cudaSuccess) return e;
   dim3 grid(a.N1 / YT, a.N0, nsys);
   LaunchScope ls(HB_KERNEL_INV_X_COMBINE, st);
@@ -176,7 +188,7 @@ template <int N0, int N1, int Q, int THREADS>
 cudaError_t launch_b(const PassArgs& a, int nslots, cudaStream_t st) {
   using C = PlaneCfg<N0, N1, Q, THREADS>;
   const size_t smem = C::SMEM_F2 * sizeof(float2);
-  cudaError_t e = ensure_smem(plane_yz_kernel<N0, N1, Q, THREADS>, smem);
+  cudaError_t e = ensure_smem<plane_yz_kernel<N0, N1, Q, THREADS>>(smem);
   if (e != cudaSuccess) return e;
   dim3 grid(2 * Q, nslots, 2 * a.N2);
   PassArgs b = a;
@@ -243,7 +255,7 @@ int yt_for(int N1) { return N1 < 16 ? N1 : 16; }
 int run_normal(const hb_plan* p, PassArgs a, cudaStream_t st) {
   const int yt = yt_for(p->N1);
   const int ia = axis_index(p->N2), iy = ilog2(yt) - 3;
-  const int nslots = a.nsys * a.ncoil;
+  const int nslots = a.nslots;
   if (nslots > 65535) return fail(HB_ERR_INVALID, "too many system x coil slots in one launch (max 65535)");
   cudaError_t e = kLaunchA[ia][iy](a, nslots, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass A: ") + cudaGetErrorString(e));
@@ -262,57 +274,359 @@ int nrr_blocks(const hb_plan* p) {
   return (int)(b < 128 ? (b < 1 ? 1 : b) : 128);
 }
 
-struct NormalWs {
-  float2* spill;
-  int* coils;
-  int* diag;
-};
-NormalWs carve_normal(Arena& ar, const hb_plan* p, int64_t nsys, int64_t ncoil) {
-  NormalWs w;
-  w.spill = ar.take<float2>((size_t)(nsys * ncoil) * spill_elems_per_slot(p));
-  w.coils = ar.take<int>((size_t)ncoil);
-  w.diag = ar.take<int>((size_t)nsys);
-  return w;
-}
-
-struct CgWs {
-  NormalWs n;
-  float2 *r, *pv, *ap;
-  double *rz, *pap, *rr;
-  int *status, *active, *iters_done;
-};
-CgWs carve_cg(Arena& ar, const hb_plan* p, int64_t nsys, int64_t ncoil, int iters) {
-  CgWs w;
-  w.n = carve_normal(ar, p, nsys, ncoil);
-  const size_t nv = (size_t)image_elems(p);
-  w.r = ar.take<float2>(nsys * nv);
-  w.pv = ar.take<float2>(nsys * nv);
-  w.ap = ar.take<float2>(nsys * nv);
-  w.rz = ar.take<double>(nsys * (size_t)(iters + 1));
-  w.pap = ar.take<double>(nsys * (size_t)npap_blocks(p));
-  w.rr = ar.take<double>(nsys * (size_t)nrr_blocks(p));
-  w.status = ar.take<int>(nsys);
-  w.active = ar.take<int>(nsys);
-  w.iters_done = ar.take<int>(nsys);
-  return w;
-}
-
 int check_plan(const hb_plan* p) {
   if (!p) return fail(HB_ERR_INVALID, "plan is NULL");
   return HB_OK;
 }
 
-int upload_indices(const int64_t* coils, int64_t ncoil, const int64_t* diag_index, int64_t s0, int64_t g,
-                   int* dcoils, int* ddiag, cudaStream_t st, std::vector<int>& hc, std::vector<int>& hd) {
-  hc.resize(ncoil);
-  for (int64_t i = 0; i < ncoil; ++i) hc[i] = (int)coils[i];
-  hd.resize(g);
-  for (int64_t i = 0; i < g; ++i) hd[i] = diag_index ? (int)diag_index[s0 + i] : 0;
-  HB_CUDA(cudaMemcpyAsync(dcoils, hc.data(), ncoil * sizeof(int), cudaMemcpyHostToDevice, st));
-  HB_CUDA(cudaMemcpyAsync(ddiag, hd.data(), g * sizeof(int), cudaMemcpyHostToDevice, st));
-  // the host vectors must outlive the copies
+// ------------------------------------------------------------- system tables ----
+// Per-group descriptor tables live in one block of the workspace and are uploaded with
+// a single copy.  Layout (byte offsets within the block) is computed identically on
+// the host.
+struct TableLayout {
+  size_t sys_x_init, sys_x_iter, sys_out, sys_smaps, sys_diag, cg_x, cg_b;  // pointer arrays
+  size_t sys_lambda;                                                          // float array
+  size_t slot_sys, slot_coil, sys_slot0, sys_nslot;                           // int arrays
+  size_t bytes;
+};
+TableLayout table_layout(int64_t g, int64_t slots) {
+  TableLayout L;
+  size_t o = 0;
+  auto take = [&](size_t n) {
+    o = (o + 15) & ~size_t(15);
+    size_t r = o;
+    o += n;
+    return r;
+  };
+  L.sys_x_init = take(8 * g);
+  L.sys_x_iter = take(8 * g);
+  L.sys_out = take(8 * g);
+  L.sys_smaps = take(8 * g);
+  L.sys_diag = take(8 * g);
+  L.cg_x = take(8 * g);
+  L.cg_b = take(8 * g);
+  L.sys_lambda = take(4 * g);
+  L.slot_sys = take(4 * slots);
+  L.slot_coil = take(4 * slots);
+  L.sys_slot0 = take(4 * g);
+  L.sys_nslot = take(4 * g);
+  L.bytes = (o + 255) & ~size_t(255);
+  return L;
+}
+
+struct GroupWs {
+  float2* spill;
+  char* tables;
+  TableLayout L;
+  // CG state (null when not a CG group)
+  float2 *r, *pv, *ap;
+  double *rz, *pap, *rr;
+  int *status, *active, *iters_done, *iter;
+};
+
+GroupWs carve_group(Arena& ar, const hb_plan* p, int64_t g, int64_t slots, int iters, bool cg) {
+  GroupWs w{};
+  w.spill = ar.take<float2>((size_t)slots * spill_elems_per_slot(p));
+  w.L = table_layout(g, slots);
+  w.tables = ar.take<char>(w.L.bytes);
+  if (cg) {
+    const size_t nv = (size_t)image_elems(p);
+    w.r = ar.take<float2>(g * nv);
+    w.pv = ar.take<float2>(g * nv);
+    w.ap = ar.take<float2>(g * nv);
+    w.rz = ar.take<double>(g * (size_t)(iters + 1));
+    w.pap = ar.take<double>(g * (size_t)npap_blocks(p));
+    w.rr = ar.take<double>(g * (size_t)nrr_blocks(p));
+    w.status = ar.take<int>(g);
+    w.active = ar.take<int>(g);
+    w.iters_done = ar.take<int>(g);
+    w.iter = ar.take<int>(1);
+  }
+  return w;
+}
+
+size_t group_bytes(const hb_plan* p, int64_t g, int64_t slots, int iters, bool cg) {
+  Arena ar(nullptr);
+  carve_group(ar, p, g, slots, iters, cg);
+  return ar.off + 256;
+}
+
+// Fills the host image of the tables of systems [s0, s0 + g) (h has L.bytes bytes).
+void fill_group_tables(char* h, const hb_plan* p, const GroupWs& w, const hb_system* sys, int64_t s0, int64_t g,
+                       bool cg) {
+  const TableLayout& L = w.L;
+  std::memset(h, 0, L.bytes);
+  auto put_ptr = [&](size_t off, int64_t i, const void* v) { std::memcpy(h + off + 8 * i, &v, 8); };
+  auto put_int = [&](size_t off, int64_t i, int v) { std::memcpy(h + off + 4 * i, &v, 4); };
+  const size_t nv = (size_t)image_elems(p);
+  int slot = 0;
+  for (int64_t i = 0; i < g; ++i) {
+    const hb_system& q = sys[s0 + i];
+    if (cg) {
+      put_ptr(L.sys_x_init, i, q.x);
+      put_ptr(L.sys_x_iter, i, w.pv + i * nv);
+      put_ptr(L.sys_out, i, w.ap + i * nv);
+      put_ptr(L.cg_x, i, q.x);
+      put_ptr(L.cg_b, i, q.b);
+    } else {
+      put_ptr(L.sys_x_init, i, q.x);
+      put_ptr(L.sys_x_iter, i, q.x);
+      put_ptr(L.sys_out, i, q.out);
+    }
+    put_ptr(L.sys_smaps, i, q.smaps);
+    put_ptr(L.sys_diag, i, q.packed_diag);
+    float lam = q.lambda;
+    std::memcpy(h + L.sys_lambda + 4 * i, &lam, 4);
+    put_int(L.sys_slot0, i, slot);
+    put_int(L.sys_nslot, i, (int)q.ncoil);
+    for (int64_t c = 0; c < q.ncoil; ++c, ++slot) {
+      put_int(L.slot_sys, slot, (int)i);
+      put_int(L.slot_coil, slot, (int)q.coils[c]);
+    }
+  }
+}
+
+// Fills and uploads the tables.  Synchronises `st` (the host image is local).
+int upload_tables(const hb_plan* p, const GroupWs& w, const hb_system* sys, int64_t s0, int64_t g, bool cg,
+                  cudaStream_t st) {
+  std::vector<char> h(w.L.bytes);
+  fill_group_tables(h.data(), p, w, sys, s0, g, cg);
+  HB_CUDA(cudaMemcpyAsync(w.tables, h.data(), w.L.bytes, cudaMemcpyHostToDevice, st));
   HB_CUDA(cudaStreamSynchronize(st));
   return HB_OK;
+}
+
+PassArgs group_pass_args(const hb_plan* p, const GroupWs& w, int64_t g, int64_t slots, bool iter_inputs) {
+  PassArgs a{};
+  a.N0 = p->N0; a.N1 = p->N1; a.N2 = p->N2;
+  a.nsys = (int)g;
+  a.nslots = (int)slots;
+  const char* t = w.tables;
+  a.slot_sys = (const int*)(t + w.L.slot_sys);
+  a.slot_coil = (const int*)(t + w.L.slot_coil);
+  a.sys_slot0 = (const int*)(t + w.L.sys_slot0);
+  a.sys_nslot = (const int*)(t + w.L.sys_nslot);
+  a.active = nullptr;
+  a.sys_x = (const float2* const*)(t + (iter_inputs ? w.L.sys_x_iter : w.L.sys_x_init));
+  a.sys_out = (float2* const*)(t + w.L.sys_out);
+  a.sys_smaps = (const float2* const*)(t + w.L.sys_smaps);
+  a.sys_diag = (const float* const*)(t + w.L.sys_diag);
+  a.sys_lambda = (const float*)(t + w.L.sys_lambda);
+  a.mul = nullptr;
+  a.spill = w.spill;
+  a.tables = p->tables;
+  a.out_ldz = (long long)p->N1 * p->N2;
+  a.out_ldy = p->N2;
+  a.accumulate = 0;
+  a.dot_partials = nullptr;
+  return a;
+}
+
+int validate_systems(const hb_plan* p, int64_t nsys, const hb_system* sys, bool cg) {
+  if (nsys < 1 || !sys) return fail(HB_ERR_INVALID, "no systems");
+  for (int64_t i = 0; i < nsys; ++i) {
+    const hb_system& q = sys[i];
+    if (!q.x || !q.smaps || !q.packed_diag || (q.ncoil > 0 && !q.coils))
+      return fail(HB_ERR_INVALID, "system " + std::to_string(i) + ": NULL pointer");
+    if (cg ? !q.b : !q.out) return fail(HB_ERR_INVALID, "system " + std::to_string(i) + ": NULL pointer");
+    if (q.ncoil < 1 || q.ncoil > 65535) return fail(HB_ERR_INVALID, "system " + std::to_string(i) + ": ncoil");
+    for (int64_t c = 0; c < q.ncoil; ++c)
+      if (q.coils[c] < 0) return fail(HB_ERR_INVALID, "system " + std::to_string(i) + ": negative coil index");
+  }
+  (void)p;
+  return HB_OK;
+}
+
+// Consecutive systems [s0, s0 + g) whose workspace fits ws_bytes (at least one system).
+int64_t next_group(const hb_plan* p, const hb_system* sys, int64_t s0, int64_t nsys, int iters, bool cg,
+                   size_t ws_bytes, int64_t* slots_out) {
+  int64_t g = 0, slots = 0;
+  while (s0 + g < nsys) {
+    const int64_t ns = slots + sys[s0 + g].ncoil;
+    if (ns > 65535 || (g > 0 && group_bytes(p, g + 1, ns, iters, cg) > ws_bytes)) break;
+    slots = ns;
+    ++g;
+  }
+  *slots_out = slots;
+  return g;
+}
+
+// ----------------------------------------------------------- graph replay state ----
+struct GraphStream {
+  bool ready = false;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e1 = nullptr, e2 = nullptr;
+};
+GraphStream g_graph_streams[64];
+std::mutex g_graph_mu;
+
+int graph_stream(int dev, GraphStream** out) {
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  if (dev < 0 || dev >= 64) return fail(HB_ERR_INVALID, "device index");
+  GraphStream& gs = g_graph_streams[dev];
+  if (!gs.ready) {
+    HB_CUDA(cudaStreamCreateWithFlags(&gs.s, cudaStreamNonBlocking));
+    HB_CUDA(cudaEventCreateWithFlags(&gs.e1, cudaEventDisableTiming));
+    HB_CUDA(cudaEventCreateWithFlags(&gs.e2, cudaEventDisableTiming));
+    gs.ready = true;
+  }
+  *out = &gs;
+  return HB_OK;
+}
+
+int launch_cg_update(int kind, void (*fn)(CgState), dim3 grid, const CgState& s, cudaStream_t st) {
+  LaunchScope ls(kind, st);
+  fn<<<grid, 256, 0, st>>>(s);
+  HB_CHECK_LAUNCH();
+  return HB_OK;
+}
+
+// One CG iteration for a group: normal op with partials, x/r update, p update, advance.
+int cg_iteration(const hb_plan* p, const PassArgs& a, const CgState& s, dim3 ugrid, int* iter, cudaStream_t st) {
+  if (int r = run_normal(p, a, st)) return r;
+  if (int r = launch_cg_update(HB_KERNEL_CG_UPDATE, cg_step_xr_kernel, ugrid, s, st)) return r;
+  if (int r = launch_cg_update(HB_KERNEL_CG_UPDATE, cg_step_p_kernel, ugrid, s, st)) return r;
+  {
+    LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
+    cg_advance_kernel<<<1, 1, 0, st>>>(iter);
+  }
+  HB_CHECK_LAUNCH();
+  return HB_OK;
+}
+constexpr int kKernelsPerCgIteration = 6;
+
+int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int iters, double tol, int flags,
+                    int32_t* status_host, int32_t* iters_done_host, void* ws, size_t ws_bytes, cudaStream_t st) {
+  if (int r = validate_systems(p, nsys, sys, true)) return r;
+  if (iters < 1) {
+    for (int64_t i = 0; i < nsys; ++i) {
+      if (status_host) status_host[i] = HB_CG_RUNNING;
+      if (iters_done_host) iters_done_host[i] = 0;
+    }
+    return HB_OK;  // ConjugateGradient::run returns immediately for iter < 1
+  }
+  const int64_t nv = image_elems(p);
+  const int nrr = nrr_blocks(p);
+  std::vector<int> stat_all(nsys), done_all(nsys);
+  const bool use_graph = (flags & HB_CG_GRAPH) && !g_prof_on.load();
+  for (int64_t s0 = 0; s0 < nsys;) {
+    int64_t slots = 0;
+    const int64_t g = next_group(p, sys, s0, nsys, iters, true, ws_bytes, &slots);
+    if (!ws || group_bytes(p, g, slots, iters, true) > ws_bytes)
+      return fail(HB_ERR_WORKSPACE, "hb_cg_run: workspace too small for one system");
+    Arena ar(ws);
+    GroupWs w = carve_group(ar, p, g, slots, iters, true);
+    if (int r = upload_tables(p, w, sys, s0, g, true, st)) return r;
+    PassArgs a = group_pass_args(p, w, g, slots, false);
+    // r = b - (A + lambda I) x
+    if (int r = run_normal(p, a, st)) return r;
+    CgState s{};
+    s.nsys = (int)g;
+    s.nv = nv;
+    s.sys_x = (float2* const*)(w.tables + w.L.cg_x);
+    s.sys_b = (const float2* const*)(w.tables + w.L.cg_b);
+    s.iter = w.iter;
+    s.r = w.r; s.p = w.pv; s.ap = w.ap;
+    s.rz = w.rz; s.rz_ld = iters + 1;
+    s.status = w.status; s.active = w.active; s.iters_done = w.iters_done;
+    s.pap_part = w.pap; s.npap = npap_blocks(p);
+    s.rr_part = w.rr;
+    s.tol = tol;
+    dim3 ugrid(nrr, (unsigned)g);
+    if (int r = launch_cg_update(HB_KERNEL_CG_UPDATE, cg_init_kernel, ugrid, s, st)) return r;
+    {
+      LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
+      cg_init_finish_kernel<<<(unsigned)g, 256, 0, st>>>(s, nrr);
+    }
+    HB_CHECK_LAUNCH();
+    PassArgs ai = group_pass_args(p, w, g, slots, true);
+    ai.active = w.active;
+    ai.dot_partials = w.pap;
+    if (!use_graph) {
+      for (int it = 0; it < iters; ++it)
+        if (int r = cg_iteration(p, ai, s, ugrid, w.iter, st)) return r;
+    } else {
+      // capture one iteration on a side stream, replay it `iters` times
+      int dev = 0;
+      HB_CUDA(cudaGetDevice(&dev));
+      GraphStream* gs = nullptr;
+      if (int r = graph_stream(dev, &gs)) return r;
+      HB_CUDA(cudaEventRecord(gs->e1, st));
+      HB_CUDA(cudaStreamWaitEvent(gs->s, gs->e1, 0));
+      cudaGraph_t graph = nullptr;
+      HB_CUDA(cudaStreamBeginCapture(gs->s, cudaStreamCaptureModeThreadLocal));
+      int rc = cg_iteration(p, ai, s, ugrid, w.iter, gs->s);
+      cudaError_t ce = cudaStreamEndCapture(gs->s, &graph);
+      if (rc) return rc;
+      if (ce != cudaSuccess) return fail(HB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      cudaGraphExec_t exec = nullptr;
+      ce = cudaGraphInstantiate(&exec, graph, 0);
+      if (ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(HB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      }
+      for (int it = 0; it < iters && ce == cudaSuccess; ++it) ce = cudaGraphLaunch(exec, gs->s);
+      g_launches.fetch_add((uint64_t)kKernelsPerCgIteration * iters, std::memory_order_relaxed);
+      cudaError_t ce2 = cudaEventRecord(gs->e2, gs->s);
+      if (ce2 == cudaSuccess) ce2 = cudaStreamWaitEvent(st, gs->e2, 0);
+      cudaGraphExecDestroy(exec);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return fail(HB_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(ce));
+      if (ce2 != cudaSuccess) return fail(HB_ERR_CUDA, std::string("graph join: ") + cudaGetErrorString(ce2));
+    }
+    HB_CUDA(cudaMemcpyAsync(stat_all.data() + s0, w.status, g * sizeof(int), cudaMemcpyDeviceToHost, st));
+    HB_CUDA(cudaMemcpyAsync(done_all.data() + s0, w.iters_done, g * sizeof(int), cudaMemcpyDeviceToHost, st));
+    HB_CUDA(cudaStreamSynchronize(st));  // the next group reuses the workspace tables
+    s0 += g;
+  }
+  HB_CUDA(cudaStreamSynchronize(st));
+  bool notpd = false;
+  for (int64_t i = 0; i < nsys; ++i) {
+    if (status_host) status_host[i] = stat_all[i];
+    if (iters_done_host) iters_done_host[i] = done_all[i];
+    if (stat_all[i] == kCgNotPD) notpd = true;
+  }
+  if (notpd) return fail(HB_ERR_NOT_PD, "A was not positive definite");
+  return HB_OK;
+}
+
+int normal_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, void* ws, size_t ws_bytes,
+                        cudaStream_t st) {
+  if (int r = validate_systems(p, nsys, sys, false)) return r;
+  for (int64_t s0 = 0; s0 < nsys;) {
+    int64_t slots = 0;
+    const int64_t g = next_group(p, sys, s0, nsys, 0, false, ws_bytes, &slots);
+    if (!ws || group_bytes(p, g, slots, 0, false) > ws_bytes)
+      return fail(HB_ERR_WORKSPACE, "hb_sense_normal_apply: workspace too small for one system");
+    Arena ar(ws);
+    GroupWs w = carve_group(ar, p, g, slots, 0, false);
+    if (int r = upload_tables(p, w, sys, s0, g, false, st)) return r;
+    PassArgs a = group_pass_args(p, w, g, slots, false);
+    if (int r = run_normal(p, a, st)) return r;
+    s0 += g;
+  }
+  return HB_OK;
+}
+
+// Builds hb_system descriptors for the contiguous-array entry points.
+std::vector<hb_system> contiguous_systems(const hb_plan* p, int64_t nsys, const void* x, void* out, const void* b,
+                                          const void* smaps, const int64_t* coils, int64_t ncoil,
+                                          const float* packed_diags, const int64_t* diag_index, float lambda) {
+  const long long nv = image_elems(p);
+  const long long pk = 8LL * nv;
+  std::vector<hb_system> v(nsys);
+  for (int64_t i = 0; i < nsys; ++i) {
+    hb_system& q = v[i];
+    q.x = const_cast<float2*>((const float2*)x + i * nv);
+    q.out = out ? (void*)((float2*)out + i * nv) : nullptr;
+    q.b = b ? (const void*)((const float2*)b + i * nv) : nullptr;
+    q.smaps = smaps;
+    q.coils = coils;
+    q.ncoil = ncoil;
+    q.packed_diag = packed_diags + (diag_index ? diag_index[i] : 0) * pk;
+    q.lambda = lambda;
+  }
+  return v;
 }
 
 // Twiddle tables (table_offsets layout), computed in FP64 on the host and rounded.
@@ -353,12 +667,15 @@ void fill_tables(float2* h, int N0, int N1, int N2) {
 constexpr int kNoAllocMaxTables = 2 * 160 + 160 + 2 * 160 + 160;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[HB_NOALLOC_SCRATCH_BYTES];
 static __device__ __align__(256) float2 g_noalloc_tables[kNoAllocMaxTables];
+constexpr int kNoAllocDescBytes = 512;  // descriptor tables of one system
+static __device__ __align__(256) unsigned char g_noalloc_desc[kNoAllocDescBytes];
 
 constexpr int kNoAllocMaxDevices = 64;
 struct NoAllocDevice {
   bool ready = false;
   void* scratch = nullptr;
   float2* tables = nullptr;
+  void* desc = nullptr;
   int dims[3] = {0, 0, 0};  // size the device's tables currently hold
 };
 NoAllocDevice g_noalloc[kNoAllocMaxDevices];
@@ -504,9 +821,12 @@ int hb_diag_build(const hb_plan* p, const float* coords, int64_t nsamples, float
 
 size_t hb_normal_workspace_bytes(const hb_plan* p, int64_t nsys, int64_t ncoil) {
   if (!p || nsys < 1 || ncoil < 1) return 0;
-  Arena ar(nullptr);
-  carve_normal(ar, p, nsys, ncoil);
-  return ar.off + 256;
+  return group_bytes(p, nsys, nsys * ncoil, 0, false);
+}
+
+size_t hb_systems_workspace_bytes(const hb_plan* p, int64_t nsys, int64_t total_coils, int iters) {
+  if (!p || nsys < 1 || total_coils < 1) return 0;
+  return group_bytes(p, nsys, total_coils, iters < 0 ? 0 : iters, iters >= 0);
 }
 
 int hb_toeplitz_apply(const hb_plan* p, const void* in, void* out, int64_t out_ldz, int64_t out_ldy, const void* mul,
@@ -516,26 +836,25 @@ int hb_toeplitz_apply(const hb_plan* p, const void* in, void* out, int64_t out_l
   if (!ws || ws_bytes < hb_normal_workspace_bytes(p, 1, 1))
     return fail(HB_ERR_WORKSPACE, "hb_toeplitz_apply: workspace too small");
   DeviceGuard dg(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t coil0 = 0;
+  hb_system q{};
+  q.x = const_cast<void*>(in);
+  q.out = out;
+  q.smaps = nullptr;
+  q.coils = &coil0;
+  q.ncoil = 1;
+  q.packed_diag = packed_diag;
+  q.lambda = 0.f;
   Arena ar(ws);
-  NormalWs w = carve_normal(ar, p, 1, 1);
-  PassArgs a{};
-  a.N0 = p->N0; a.N1 = p->N1; a.N2 = p->N2;
-  a.nsys = 1; a.ncoil = 1;
-  a.coils = nullptr; a.diag_of_sys = nullptr; a.active = nullptr;
-  a.x = (const float2*)in;
-  a.smaps = nullptr;
+  GroupWs w = carve_group(ar, p, 1, 1, 0, false);
+  if (int r = upload_tables(p, w, &q, 0, 1, false, st)) return r;
+  PassArgs a = group_pass_args(p, w, 1, 1, false);
   a.mul = (const float2*)mul;
-  a.spill = w.spill;
-  a.diag = packed_diag;
-  a.tables = p->tables;
-  a.out = (float2*)out;
-  a.out_sys_stride = 0;
   a.out_ldz = out_ldz;
   a.out_ldy = out_ldy;
   a.accumulate = accumulate ? 1 : 0;
-  a.lambda = 0.f;
-  a.dot_partials = nullptr;
-  return run_normal(p, a, (cudaStream_t)stream);
+  return run_normal(p, a, st);
 }
 
 int hb_sense_normal_apply(const hb_plan* p, int64_t nsys, const void* x, void* out, const void* smaps,
@@ -544,47 +863,22 @@ int hb_sense_normal_apply(const hb_plan* p, int64_t nsys, const void* x, void* o
   if (int r = check_plan(p)) return r;
   if (nsys < 1 || ncoil < 1) return fail(HB_ERR_INVALID, "hb_sense_normal_apply: nsys and ncoil must be >= 1");
   if (!x || !out || !smaps || !coils || !packed_diags) return fail(HB_ERR_INVALID, "hb_sense_normal_apply: NULL pointer");
-  const size_t one = hb_normal_workspace_bytes(p, 1, ncoil);
-  if (!ws || ws_bytes < one) return fail(HB_ERR_WORKSPACE, "hb_sense_normal_apply: workspace too small");
   DeviceGuard dg(p->device);
-  cudaStream_t st = (cudaStream_t)stream;
-  int64_t g = nsys;
-  while (g > 1 && hb_normal_workspace_bytes(p, g, ncoil) > ws_bytes) g = (g + 1) / 2;
-  while (g * ncoil > 65535) g = (g + 1) / 2;
-  const long long nv = image_elems(p);
-  std::vector<int> hc, hd;
-  for (int64_t s0 = 0; s0 < nsys; s0 += g) {
-    const int64_t gg = (nsys - s0) < g ? (nsys - s0) : g;
-    Arena ar(ws);
-    NormalWs w = carve_normal(ar, p, gg, ncoil);
-    if (int r = upload_indices(coils, ncoil, diag_index, s0, gg, w.coils, w.diag, st, hc, hd)) return r;
-    PassArgs a{};
-    a.N0 = p->N0; a.N1 = p->N1; a.N2 = p->N2;
-    a.nsys = (int)gg; a.ncoil = (int)ncoil;
-    a.coils = w.coils; a.diag_of_sys = w.diag; a.active = nullptr;
-    a.x = (const float2*)x + s0 * nv;
-    a.smaps = (const float2*)smaps;
-    a.mul = nullptr;
-    a.spill = w.spill;
-    a.diag = packed_diags;
-    a.tables = p->tables;
-    a.out = (float2*)out + s0 * nv;
-    a.out_sys_stride = nv;
-    a.out_ldz = (long long)p->N1 * p->N2;
-    a.out_ldy = p->N2;
-    a.accumulate = 0;
-    a.lambda = lambda;
-    a.dot_partials = nullptr;
-    if (int r = run_normal(p, a, st)) return r;
-  }
-  return HB_OK;
+  std::vector<hb_system> v =
+      contiguous_systems(p, nsys, x, out, nullptr, smaps, coils, ncoil, packed_diags, diag_index, lambda);
+  return normal_systems_impl(p, nsys, v.data(), ws, ws_bytes, (cudaStream_t)stream);
+}
+
+int hb_sense_normal_apply_systems(const hb_plan* p, int64_t nsys, const hb_system* systems, void* ws,
+                                  size_t ws_bytes, void* stream) {
+  if (int r = check_plan(p)) return r;
+  DeviceGuard dg(p->device);
+  return normal_systems_impl(p, nsys, systems, ws, ws_bytes, (cudaStream_t)stream);
 }
 
 size_t hb_cg_workspace_bytes(const hb_plan* p, int64_t nsys, int64_t ncoil, int iters) {
   if (!p || nsys < 1 || ncoil < 1 || iters < 0) return 0;
-  Arena ar(nullptr);
-  carve_cg(ar, p, nsys, ncoil, iters);
-  return ar.off + 256;
+  return group_bytes(p, nsys, nsys * ncoil, iters, true);
 }
 
 int hb_cg_run(const hb_plan* p, int64_t nsys, void* x, const void* b, const void* smaps, const int64_t* coils,
@@ -593,98 +887,19 @@ int hb_cg_run(const hb_plan* p, int64_t nsys, void* x, const void* b, const void
   if (int r = check_plan(p)) return r;
   if (nsys < 1 || ncoil < 1) return fail(HB_ERR_INVALID, "hb_cg_run: nsys and ncoil must be >= 1");
   if (!x || !b || !smaps || !coils || !packed_diags) return fail(HB_ERR_INVALID, "hb_cg_run: NULL pointer");
-  if (iters < 1) {
-    for (int64_t s = 0; s < nsys; ++s) {
-      if (status_host) status_host[s] = HB_CG_RUNNING;
-      if (iters_done_host) iters_done_host[s] = 0;
-    }
-    return HB_OK;  // ConjugateGradient::run returns immediately for iter < 1
-  }
-  if (!ws || ws_bytes < hb_cg_workspace_bytes(p, 1, ncoil, iters))
-    return fail(HB_ERR_WORKSPACE, "hb_cg_run: workspace too small");
   DeviceGuard dg(p->device);
-  cudaStream_t st = (cudaStream_t)stream;
-  int64_t g = nsys;
-  while (g > 1 && hb_cg_workspace_bytes(p, g, ncoil, iters) > ws_bytes) g = (g + 1) / 2;
-  while (g * ncoil > 65535) g = (g + 1) / 2;
-  const long long nv = image_elems(p);
-  const int nrr = nrr_blocks(p);
-  std::vector<int> hc, hd;
-  std::vector<int> stat_all(nsys), done_all(nsys);
-  for (int64_t s0 = 0; s0 < nsys; s0 += g) {
-    const int64_t gg = (nsys - s0) < g ? (nsys - s0) : g;
-    Arena ar(ws);
-    CgWs w = carve_cg(ar, p, gg, ncoil, iters);
-    if (int r = upload_indices(coils, ncoil, diag_index, s0, gg, w.n.coils, w.n.diag, st, hc, hd)) return r;
-    PassArgs a{};
-    a.N0 = p->N0; a.N1 = p->N1; a.N2 = p->N2;
-    a.nsys = (int)gg; a.ncoil = (int)ncoil;
-    a.coils = w.n.coils; a.diag_of_sys = w.n.diag; a.active = nullptr;
-    a.x = (const float2*)x + s0 * nv;
-    a.smaps = (const float2*)smaps;
-    a.mul = nullptr;
-    a.spill = w.n.spill;
-    a.diag = packed_diags;
-    a.tables = p->tables;
-    a.out = w.ap;
-    a.out_sys_stride = nv;
-    a.out_ldz = (long long)p->N1 * p->N2;
-    a.out_ldy = p->N2;
-    a.accumulate = 0;
-    a.lambda = lambda;
-    a.dot_partials = nullptr;
-    // r = b - (A + lambda I) x
-    if (int r = run_normal(p, a, st)) return r;
-    CgState s{};
-    s.nsys = (int)gg;
-    s.nv = nv;
-    s.x = (float2*)x + s0 * nv;
-    s.b = (const float2*)b + s0 * nv;
-    s.r = w.r; s.p = w.pv; s.ap = w.ap;
-    s.rz = w.rz; s.rz_ld = iters + 1;
-    s.status = w.status; s.active = w.active; s.iters_done = w.iters_done;
-    s.pap_part = w.pap; s.npap = npap_blocks(p);
-    s.rr_part = w.rr;
-    s.tol = tol;
-    dim3 ugrid(nrr, (unsigned)gg);
-    {
-      LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
-      cg_init_kernel<<<ugrid, 256, 0, st>>>(s);
-    }
-    HB_CHECK_LAUNCH();
-    {
-      LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
-      cg_init_finish_kernel<<<(unsigned)gg, 256, 0, st>>>(s, nrr);
-    }
-    HB_CHECK_LAUNCH();
-    a.x = w.pv;
-    a.active = w.active;
-    a.dot_partials = w.pap;
-    for (int it = 0; it < iters; ++it) {
-      if (int r = run_normal(p, a, st)) return r;
-      {
-        LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
-        cg_step_xr_kernel<<<ugrid, 256, 0, st>>>(s, it);
-      }
-      HB_CHECK_LAUNCH();
-      {
-        LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
-        cg_step_p_kernel<<<ugrid, 256, 0, st>>>(s, it);
-      }
-      HB_CHECK_LAUNCH();
-    }
-    HB_CUDA(cudaMemcpyAsync(stat_all.data() + s0, w.status, gg * sizeof(int), cudaMemcpyDeviceToHost, st));
-    HB_CUDA(cudaMemcpyAsync(done_all.data() + s0, w.iters_done, gg * sizeof(int), cudaMemcpyDeviceToHost, st));
-  }
-  HB_CUDA(cudaStreamSynchronize(st));
-  bool notpd = false;
-  for (int64_t s = 0; s < nsys; ++s) {
-    if (status_host) status_host[s] = stat_all[s];
-    if (iters_done_host) iters_done_host[s] = done_all[s];
-    if (stat_all[s] == kCgNotPD) notpd = true;
-  }
-  if (notpd) return fail(HB_ERR_NOT_PD, "A was not positive definite");
-  return HB_OK;
+  std::vector<hb_system> v =
+      contiguous_systems(p, nsys, x, nullptr, b, smaps, coils, ncoil, packed_diags, diag_index, lambda);
+  return cg_systems_impl(p, nsys, v.data(), iters, tol, 0, status_host, iters_done_host, ws, ws_bytes,
+                         (cudaStream_t)stream);
+}
+
+int hb_cg_run_systems(const hb_plan* p, int64_t nsys, const hb_system* systems, int iters, double tol, int flags,
+                      int32_t* status_host, int32_t* iters_done_host, void* ws, size_t ws_bytes, void* stream) {
+  if (int r = check_plan(p)) return r;
+  DeviceGuard dg(p->device);
+  return cg_systems_impl(p, nsys, systems, iters, tol, flags, status_host, iters_done_host, ws, ws_bytes,
+                         (cudaStream_t)stream);
 }
 
 int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in, void* out, int64_t out_ldz,
@@ -709,6 +924,7 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
   if (!d.ready) {  // once per device, with that device current
     HB_CUDA(cudaGetSymbolAddress(&d.scratch, g_noalloc_scratch));
     HB_CUDA(cudaGetSymbolAddress((void**)&d.tables, g_noalloc_tables));
+    HB_CUDA(cudaGetSymbolAddress(&d.desc, g_noalloc_desc));
     d.ready = true;
   }
   if (d.dims[0] != nz || d.dims[1] != ny || d.dims[2] != nx) {
@@ -728,23 +944,29 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
   p.device = dev;
   p.tables = d.tables;
   p.to = table_offsets(p.N0, p.N1, p.N2);
-  PassArgs a{};
-  a.N0 = p.N0; a.N1 = p.N1; a.N2 = p.N2;
-  a.nsys = 1; a.ncoil = 1;
-  a.coils = nullptr; a.diag_of_sys = nullptr; a.active = nullptr;
-  a.x = (const float2*)in;
-  a.smaps = nullptr;
+  // one system, one unit coil: its descriptor tables go to the built-in table block
+  const int64_t coil0 = 0;
+  hb_system q{};
+  q.x = const_cast<void*>(in);
+  q.out = out;
+  q.smaps = nullptr;
+  q.coils = &coil0;
+  q.ncoil = 1;
+  q.packed_diag = packed_diag;
+  q.lambda = 0.f;
+  GroupWs w{};
+  w.spill = (float2*)d.scratch;
+  w.L = table_layout(1, 1);
+  w.tables = (char*)d.desc;
+  char h[kNoAllocDescBytes];  // host stack, no heap
+  fill_group_tables(h, &p, w, &q, 0, 1, false);
+  HB_CUDA(cudaMemcpyAsync(w.tables, h, w.L.bytes, cudaMemcpyHostToDevice, st));
+  HB_CUDA(cudaStreamSynchronize(st));
+  PassArgs a = group_pass_args(&p, w, 1, 1, false);
   a.mul = (const float2*)mul;
-  a.spill = (float2*)d.scratch;
-  a.diag = packed_diag;
-  a.tables = d.tables;
-  a.out = (float2*)out;
-  a.out_sys_stride = 0;
   a.out_ldz = out_ldz;
   a.out_ldy = out_ldy;
   a.accumulate = accumulate ? 1 : 0;
-  a.lambda = 0.f;
-  a.dot_partials = nullptr;
   return run_normal(&p, a, st);
 }
 

@@ -20,9 +20,10 @@ enum CgStatus : int { kCgRunning = 0, kCgConverged = 1, kCgNotPD = 2 };
 
 struct CgState {
   int nsys;
-  long long nv;          // elements per system
-  float2* x;             // [nsys][nv] solution (caller)
-  const float2* b;       // [nsys][nv] right-hand side (caller)
+  long long nv;               // elements per system
+  float2* const* sys_x;       // [nsys] solution of each system (caller buffers)
+  const float2* const* sys_b; // [nsys] right-hand side of each system (caller buffers)
+  int* iter;                  // current iteration (device counter, advanced by cg_advance)
   float2* r;             // [nsys][nv]
   float2* p;             // [nsys][nv]
   float2* ap;            // [nsys][nv]
@@ -74,8 +75,9 @@ __global__ void __launch_bounds__(256) cg_init_kernel(CgState s) {
   const int sys = blockIdx.y;
   const long long base = (long long)sys * s.nv;
   double acc = 0.0;
+  const float2* b = s.sys_b[sys];
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x) {
-    const float2 r = csub(s.b[base + i], s.ap[base + i]);
+    const float2 r = csub(b[i], s.ap[base + i]);
     s.r[base + i] = r;
     s.p[base + i] = r;
     acc += (double)r.x * r.x + (double)r.y * r.y;
@@ -89,6 +91,7 @@ __global__ void __launch_bounds__(256) cg_init_finish_kernel(CgState s, int nrr)
   const int sys = blockIdx.x;
   const double rz = block_sum_fixed(s.rr_part + (long long)sys * nrr, nrr, red);
   if (threadIdx.x == 0) {
+    if (sys == 0) *s.iter = 0;
     s.rz[(long long)sys * s.rz_ld] = rz;
     s.iters_done[sys] = 0;
     const bool run = !(sqrt(rz) < s.tol);
@@ -97,10 +100,11 @@ __global__ void __launch_bounds__(256) cg_init_finish_kernel(CgState s, int nrr)
   }
 }
 
-__global__ void __launch_bounds__(256) cg_step_xr_kernel(CgState s, int it) {
+__global__ void __launch_bounds__(256) cg_step_xr_kernel(CgState s) {
   __shared__ double red[32];
   const int sys = blockIdx.y;
   if (!s.active[sys]) return;
+  const int it = *s.iter;
   const double pap = block_sum_fixed(s.pap_part + (long long)sys * s.npap, s.npap, red);
   if (!(pap > 0.0)) {  // also catches NaN
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -112,27 +116,29 @@ __global__ void __launch_bounds__(256) cg_step_xr_kernel(CgState s, int it) {
   const double alpha = s.rz[(long long)sys * s.rz_ld + it] / pap;
   const float af = (float)alpha;
   const long long base = (long long)sys * s.nv;
+  float2* xv = s.sys_x[sys];
   double acc = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x) {
     const float2 p = s.p[base + i];
     const float2 ap = s.ap[base + i];
-    float2 x = s.x[base + i];
+    float2 x = xv[i];
     float2 r = s.r[base + i];
     x.x = fmaf(af, p.x, x.x);
     x.y = fmaf(af, p.y, x.y);
     r.x = fmaf(-af, ap.x, r.x);
     r.y = fmaf(-af, ap.y, r.y);
-    s.x[base + i] = x;
+    xv[i] = x;
     s.r[base + i] = r;
     acc += (double)r.x * r.x + (double)r.y * r.y;
   }
   block_write_partial(acc, s.rr_part + (long long)sys * gridDim.x + blockIdx.x, red);
 }
 
-__global__ void __launch_bounds__(256) cg_step_p_kernel(CgState s, int it) {
+__global__ void __launch_bounds__(256) cg_step_p_kernel(CgState s) {
   __shared__ double red[32];
   const int sys = blockIdx.y;
   if (!s.active[sys]) return;
+  const int it = *s.iter;
   const double rznew = block_sum_fixed(s.rr_part + (long long)sys * gridDim.x, gridDim.x, red);
   const double rzold = s.rz[(long long)sys * s.rz_ld + it];
   const float beta = (float)(rznew / rzold);
@@ -153,5 +159,8 @@ __global__ void __launch_bounds__(256) cg_step_p_kernel(CgState s, int it) {
     }
   }
 }
+
+// Ends an iteration: every kernel of the next one reads the advanced counter.
+__global__ void cg_advance_kernel(int* iter) { *iter += 1; }
 
 }  // namespace hb

@@ -107,25 +107,30 @@ __host__ __device__ inline TableOffsets table_offsets(int N0, int N1, int N2) {
   return o;
 }
 
-// Problem descriptor shared by the passes.
+// Problem descriptor shared by the passes.  Systems are described by per-system tables
+// so that one launch sequence can carry systems of different jobs (own buffers, coil
+// maps, coil counts, diagonals, lambda).  A slot is one (system, coil) pair; the slots
+// of a system are consecutive.
 struct PassArgs {
   int N0, N1, N2;
-  int nsys, ncoil;              // slots = nsys * ncoil
-  const int* coils;             // [ncoil] coil index into smaps (device)
-  const int* diag_of_sys;       // [nsys] diagonal index per system (device)
-  const int* active;            // [nsys] nonzero = process this system (device, nullable)
-  const float2* x;              // [nsys][N0][N1][N2]
-  const float2* smaps;          // [*][N0][N1][N2] (nullable -> S = 1)
-  const float2* mul;            // [N0][N1][N2] unconjugated multiplier (nullable)
-  float2* spill;                // [nsys*ncoil][M2][N0][N1]
-  const float* diag;            // packed diagonals [ndiag][M2][2][N1][M0]
-  const float2* tables;         // twiddle tables, see table_offsets
-  float2* out;                  // output base
-  long long out_sys_stride, out_ldz, out_ldy;  // element strides of out
-  int accumulate;               // 1: out += result, 0: out = result
-  float lambda;                 // adds lambda * x
-  double* dot_partials;         // [nsys][nblocks_c] Re<x, out> partials (nullable)
-  int prefetch_ahead;           // plane pass: L2-prefetch distance in clusters (0 = off)
+  int nsys, nslots;
+  const int* slot_sys;             // [nslots] system of the slot
+  const int* slot_coil;            // [nslots] coil index into that system's coil maps
+  const int* sys_slot0;            // [nsys] first slot of the system
+  const int* sys_nslot;            // [nsys] number of coils of the system
+  const int* active;               // [nsys] nonzero = process this system (nullable)
+  const float2* const* sys_x;      // [nsys] input image [N0][N1][N2]
+  float2* const* sys_out;          // [nsys] output image (strides out_ldz, out_ldy, 1)
+  const float2* const* sys_smaps;  // [nsys] coil maps [*][N0][N1][N2]; a null entry = unit map
+  const float* const* sys_diag;    // [nsys] packed diagonal [M2][2][N1][M0]
+  const float* sys_lambda;         // [nsys] adds lambda * x (nullable = 0)
+  const float2* mul;               // [N0][N1][N2] unconjugated multiplier (single system, nullable)
+  float2* spill;                   // [nslots][M2][N0][N1]
+  const float2* tables;            // twiddle tables, see table_offsets
+  long long out_ldz, out_ldy;      // element strides of every output image
+  int accumulate;                  // 1: out += result, 0: out = result
+  double* dot_partials;            // [nsys][nblocks_c] Re<x, out> partials (nullable)
+  int prefetch_ahead;              // plane pass: L2-prefetch distance in clusters (0 = off)
 };
 
 // ------------------------------------------------------------------------ pass A ----
@@ -140,9 +145,9 @@ expand_fwd_x_kernel(PassArgs a) {
   float2* tw = xbuf + C::NTEAMS * C::TBUF;      // [M2]
 
   const int slot = blockIdx.z;
-  const int sys = slot / a.ncoil;
+  const int sys = a.slot_sys[slot];
   if (a.active && !a.active[sys]) return;
-  const int coil = a.coils ? a.coils[slot % a.ncoil] : 0;
+  const int coil = a.slot_coil[slot];
   const int z = blockIdx.y;
   const int y0 = blockIdx.x * YT;
   const int N0 = a.N0, N1 = a.N1;
@@ -153,8 +158,9 @@ expand_fwd_x_kernel(PassArgs a) {
   const int team = threadIdx.x / S, t = threadIdx.x % S;
   float2* buf = xbuf + team * C::TBUF;
   const long long plane = (long long)N1 * N2;
-  const float2* xs = a.x + (long long)sys * N0 * plane + (long long)z * plane;
-  const float2* ss = a.smaps ? a.smaps + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
+  const float2* xs = a.sys_x[sys] + (long long)z * plane;
+  const float2* sm = a.sys_smaps[sys];
+  const float2* ss = sm ? sm + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
 
 #pragma unroll 1
   for (int it = 0; it < C::LPT; ++it) {
@@ -203,7 +209,7 @@ plane_yz_kernel(PassArgs a) {
   const int q = rank % Q;  // owned column / row block
   const int slot = blockIdx.y;
   const int kx = blockIdx.z;
-  const int sys = slot / a.ncoil;
+  const int sys = a.slot_sys[slot];
   if (a.active && !a.active[sys]) return;  // uniform for the whole cluster
   const int M2 = 2 * a.N2;
 
@@ -216,7 +222,7 @@ plane_yz_kernel(PassArgs a) {
   __syncthreads();
 
   float2* g = a.spill + ((long long)slot * M2 + kx) * N0 * N1;
-  const float* T = a.diag + ((((long long)(a.diag_of_sys ? a.diag_of_sys[sys] : 0) * M2 + kx) * 2 + h) * N1) * M0;
+  const float* T = a.sys_diag[sys] + (((long long)kx * 2 + h) * N1) * M0;
   float2* Pr[Q];  // column blocks of this parity, one per cluster rank h*Q + q'
 #pragma unroll
   for (int qq = 0; qq < Q; ++qq) Pr[qq] = cluster.map_shared_rank(P, h * Q + qq);
@@ -388,9 +394,10 @@ inv_x_combine_kernel(PassArgs a) {
   const long long plane = (long long)N1 * N2;
   const long long slot_stride = (long long)M2 * N0 * N1;
 
+  const int slot0 = a.sys_slot0[sys], ncoil = a.sys_nslot[sys];
   // asynchronous copy of coil ci's [kx][y] tile into tiles[ci & 1]
   auto prefetch = [&](int ci) {
-    const float2* src = a.spill + (long long)(sys * a.ncoil + ci) * slot_stride + (long long)z * N1 + y0;
+    const float2* src = a.spill + (long long)(slot0 + ci) * slot_stride + (long long)z * N1 + y0;
     float2* dst = tiles + (ci & 1) * M2 * C::TILE_LD;
     for (int i = threadIdx.x; i < M2 * YT; i += C::THREADS) {
       const int kx = i / YT, j = i % YT;
@@ -405,18 +412,19 @@ inv_x_combine_kernel(PassArgs a) {
 #pragma unroll
     for (int e = 0; e < E / 2; ++e) acc[l][e] = make_float2(0.f, 0.f);
 
-  prefetch(0);
+  const float2* sm = a.sys_smaps[sys];
+  if (ncoil > 0) prefetch(0);
 #pragma unroll 1
-  for (int ci = 0; ci < a.ncoil; ++ci) {
-    if (ci + 1 < a.ncoil) {
+  for (int ci = 0; ci < ncoil; ++ci) {
+    if (ci + 1 < ncoil) {
       prefetch(ci + 1);
       cp_async_wait<1>();  // coil ci's tile has landed
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    const int coil = a.coils ? a.coils[ci] : 0;
-    const float2* ss = a.smaps ? a.smaps + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
+    const int coil = a.slot_coil[slot0 + ci];
+    const float2* ss = sm ? sm + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
     const float2* tile = tiles + (ci & 1) * M2 * C::TILE_LD;
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
@@ -444,7 +452,9 @@ inv_x_combine_kernel(PassArgs a) {
 
   // epilogue
   double dot = 0.0;
-  const float2* xs = a.x + (long long)sys * N0 * plane + (long long)z * plane;
+  const float2* xs = a.sys_x[sys] + (long long)z * plane;
+  float2* outp = a.sys_out[sys];
+  const float lambda = a.sys_lambda ? a.sys_lambda[sys] : 0.f;
 #pragma unroll
   for (int l = 0; l < LPT; ++l) {
     const int y = y0 + team + l * C::NTEAMS;
@@ -453,8 +463,8 @@ inv_x_combine_kernel(PassArgs a) {
       const int xi = din_index<M2>(t, e);
       float2 val = acc[l][e];
       const float2 xv = xs[(long long)y * N2 + xi];
-      if (a.lambda != 0.f) val = make_float2(fmaf(a.lambda, xv.x, val.x), fmaf(a.lambda, xv.y, val.y));
-      float2* o = a.out + sys * a.out_sys_stride + z * a.out_ldz + y * a.out_ldy + xi;
+      if (lambda != 0.f) val = make_float2(fmaf(lambda, xv.x, val.x), fmaf(lambda, xv.y, val.y));
+      float2* o = outp + z * a.out_ldz + y * a.out_ldy + xi;
       if (a.accumulate) val = cadd(*o, val);
       *o = val;
       dot += (double)xv.x * (double)val.x + (double)xv.y * (double)val.y;

@@ -43,6 +43,19 @@ def _check_c64(t, name, device, shape=None):
         raise RuntimeError(f"{name} has shape {tuple(t.shape)}, expected (..., {shape})")
 
 
+class System:
+    """One system of a heterogeneous batch (``struct hb_system``).
+
+    x: image [nz, ny, nx] (CG: initial guess, overwritten with the solution); out: the
+    normal-op output; b: CG right-hand side; smaps: this system's coil maps; coils:
+    indices into them (default all); packed: this system's packed diagonal (1-D view);
+    lam: adds lam * x."""
+
+    def __init__(self, x, smaps, packed, out=None, b=None, coils=None, lam=0.0):
+        self.x, self.out, self.b, self.smaps, self.packed, self.lam = x, out, b, smaps, packed, float(lam)
+        self.coils = list(range(smaps.shape[0])) if coils is None else [int(c) for c in coils]
+
+
 class ToeplitzPlan:
     """Geometry of an nz x ny x nx image and its 2x Toeplitz grid on one CUDA device."""
 
@@ -214,6 +227,65 @@ class ToeplitzPlan:
         code = self.lib.hb_cg_run(self._h, nsys, _ptr(x4), _ptr(b4), _ptr(smaps), ca, len(coils), _ptr(packed), da,
                                   float(lam), int(iters), float(tol), status, done, _ptr(ws), nb,
                                   _stream_ptr(self.device))
+        if code == capi.HB_ERR_NOT_PD and not raise_not_pd:
+            return list(status), list(done)
+        capi.check(code)
+        return list(status), list(done)
+
+    # ------------------------------------------------------- heterogeneous batch ----
+    def _systems(self, systems, cg):
+        arr = (capi.HbSystem * len(systems))()
+        keep = []
+        for i, q in enumerate(systems):
+            _check_c64(q.x, "x", self.device, self.shape)
+            _check_c64(q.smaps, "smaps", self.device, self.shape)
+            if cg:
+                _check_c64(q.b, "b", self.device, self.shape)
+            else:
+                _check_c64(q.out, "out", self.device, self.shape)
+            if q.packed.dtype != torch.float32 or q.packed.numel() != self.packed_numel() or \
+                    not q.packed.is_contiguous() or q.packed.device != self.device:
+                raise RuntimeError("each system needs one contiguous float32 packed diagonal on the device")
+            if any(c < 0 or c >= q.smaps.shape[0] for c in q.coils) or not q.coils:
+                raise RuntimeError("coil index out of range")
+            ca = capi.i64_array(q.coils)
+            keep.append(ca)
+            arr[i].x = q.x.data_ptr()
+            arr[i].out = q.out.data_ptr() if q.out is not None else None
+            arr[i].b = q.b.data_ptr() if q.b is not None else None
+            arr[i].smaps = q.smaps.data_ptr()
+            arr[i].coils = ca
+            arr[i].ncoil = len(q.coils)
+            arr[i].packed_diag = q.packed.data_ptr()
+            arr[i].lam = q.lam
+        return arr, keep
+
+    def sense_normal_systems(self, systems, workspace_bytes=None):
+        """out = (A^H A)_toep x + lam x for every System, in as few launch sequences as the workspace allows."""
+        arr, keep = self._systems(systems, cg=False)
+        ncoil = sum(len(q.coils) for q in systems)
+        nb = self.lib.hb_systems_workspace_bytes(self._h, len(systems), ncoil, -1)
+        if workspace_bytes is not None:
+            nb = min(nb, int(workspace_bytes))
+        ws = self._workspace(nb)
+        capi.check(self.lib.hb_sense_normal_apply_systems(self._h, len(systems), arr, _ptr(ws), nb,
+                                                          _stream_ptr(self.device)))
+
+    def cg_systems(self, systems, iters=30, tol=0.0, graph=True, workspace_bytes=None, raise_not_pd=True):
+        """Batched CG over heterogeneous systems; each System's x is updated in place.
+        graph=True captures each iteration as a CUDA graph and replays it."""
+        arr, keep = self._systems(systems, cg=True)
+        n = len(systems)
+        ncoil = sum(len(q.coils) for q in systems)
+        nb = self.lib.hb_systems_workspace_bytes(self._h, n, ncoil, int(iters))
+        if workspace_bytes is not None:
+            nb = min(nb, int(workspace_bytes))
+        ws = self._workspace(max(nb, 1))
+        status = (ctypes.c_int32 * n)()
+        done = (ctypes.c_int32 * n)()
+        code = self.lib.hb_cg_run_systems(self._h, n, arr, int(iters), float(tol),
+                                          capi.HB_CG_GRAPH if graph else 0, status, done, _ptr(ws), nb,
+                                          _stream_ptr(self.device))
         if code == capi.HB_ERR_NOT_PD and not raise_not_pd:
             return list(status), list(done)
         capi.check(code)

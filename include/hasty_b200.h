@@ -108,6 +108,43 @@ int hb_sense_normal_apply(const hb_plan* plan, int64_t nsys, const void* x, void
                           const float* packed_diags, const int64_t* diag_index, float lambda,
                           void* workspace, size_t workspace_bytes, void* stream);
 
+/* One system of a heterogeneous batch (jobs with their own buffers, coil maps, coil
+ * lists, diagonals and lambda).  All pointers are device pointers except `coils` (host).
+ *   x      normal op: input image; CG: initial guess in, solution out
+ *   out    normal op: output image (must not alias another system's x); CG: unused
+ *   b      CG: right-hand side; normal op: unused
+ *   smaps  this system's coil maps [*][nz][ny][nx]; coils[0..ncoil) index into them
+ *   packed_diag  this system's packed diagonal; lambda adds lambda * x */
+typedef struct hb_system {
+  void* x;
+  void* out;
+  const void* b;
+  const void* smaps;
+  const int64_t* coils;
+  int64_t ncoil;
+  const float* packed_diag;
+  float lambda;
+} hb_system;
+
+/* Workspace bytes for nsys systems with total_coils (system, coil) pairs handled in one
+ * launch sequence: normal op when iters < 0, CG with `iters` iterations otherwise. */
+size_t hb_systems_workspace_bytes(const hb_plan* plan, int64_t nsys, int64_t total_coils, int iters);
+
+/* The Toeplitz SENSE normal op over a heterogeneous batch (BatchedSenseNormal::apply,
+ * lib/mri/batch_sense.cpp:349-450, with per-outer-batch coil lists).  Systems are
+ * processed in groups that fit the workspace, each group in one launch sequence. */
+int hb_sense_normal_apply_systems(const hb_plan* plan, int64_t nsys, const hb_system* systems,
+                                  void* workspace, size_t workspace_bytes, void* stream);
+
+/* Capture each CG iteration of a group as a CUDA graph and replay it (hb_cg_run_systems). */
+#define HB_CG_GRAPH 1
+
+/* Batched CG over a heterogeneous batch (BatchedConjugateGradient::run,
+ * lib/op/opalgs.ixx:93-121); same semantics and return codes as hb_cg_run. */
+int hb_cg_run_systems(const hb_plan* plan, int64_t nsys, const hb_system* systems, int iters,
+                      double tol, int flags, int32_t* status_host, int32_t* iters_done_host,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* Workspace bytes of hb_cg_run for nsys systems handled at once. */
 size_t hb_cg_workspace_bytes(const hb_plan* plan, int64_t nsys, int64_t ncoil, int iters);
 

@@ -259,3 +259,67 @@ def test_sense_normal_non_power_of_two(cuda, shape, ncoil):
     plan.sense_normal(_c64(x, cuda), out, _c64(sm, cuda), packed, lam=1e-3)
     ref = O.sense_normal_toeplitz(x, sm, T) + 1e-3 * x
     assert O.rel_l2(_np(out), ref) < TOL
+
+
+def _mixed_jobs(plan, cuda, seeds, ncoils, lam=1e-3):
+    from hastycompute_b200.toeplitz import System
+    shape = plan.shape
+    jobs = []
+    for seed, nc in zip(seeds, ncoils):
+        rng = np.random.default_rng(seed)
+        T = O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 800)), shape)
+        sm = synth.coil_maps(nc + 1, shape, seed=seed)
+        coils = list(range(nc + 1))[1:] if nc % 2 else list(range(nc))
+        xt = synth.gaussian_image(shape, seed=seed + 100)
+        b = O.sense_normal_toeplitz(xt, sm, T, coils) + lam * xt
+        jobs.append(dict(T=T, sm=sm, coils=coils, b=b, packed=plan.pack_diagonal(_c64(T, cuda)),
+                         smt=_c64(sm, cuda), bt=_c64(b, cuda), lam=lam, x=xt))
+    return jobs
+
+
+def test_heterogeneous_systems_normal_and_cg(cuda):
+    """Systems of different jobs (own buffers, coil maps, coil counts, diagonals) in one
+    launch sequence, against the FP64 oracle; graph and plain CG agree bitwise."""
+    from hastycompute_b200.toeplitz import System
+    shape = (16, 16, 32)
+    plan = ToeplitzPlan(shape, cuda)
+    jobs = _mixed_jobs(plan, cuda, [1, 2, 3], [3, 5, 2])
+    # normal op
+    systems, outs = [], []
+    for j in jobs:
+        out = torch.empty(shape, dtype=torch.complex64, device=cuda)
+        outs.append(out)
+        systems.append(System(_c64(j["x"], cuda), j["smt"], j["packed"], out=out, coils=j["coils"], lam=j["lam"]))
+    plan.sense_normal_systems(systems)
+    for j, out in zip(jobs, outs):
+        assert O.rel_l2(_np(out), j["b"]) < TOL
+    # CG, plain and graph-replayed
+    res = {}
+    for graph in (False, True):
+        xs = [torch.zeros(shape, dtype=torch.complex64, device=cuda) for _ in jobs]
+        sys_cg = [System(x, j["smt"], j["packed"], b=j["bt"], coils=j["coils"], lam=j["lam"]) for x, j in zip(xs, jobs)]
+        status, done = plan.cg_systems(sys_cg, iters=8, graph=graph)
+        assert done == [8] * len(jobs)
+        res[graph] = xs
+    for a, b in zip(res[False], res[True]):
+        assert torch.equal(a, b)
+    for j, x in zip(jobs, res[True]):
+        A = O.regularized(lambda v, j=j: O.sense_normal_toeplitz(v, j["sm"], j["T"], j["coils"]), j["lam"])
+        xo, _ = O.conjugate_gradient(A, j["b"], iters=8)
+        assert O.rel_l2(_np(x), xo) < 1e-4
+
+
+def test_result_same_alone_and_in_the_mix(cuda):
+    """A job solved alone and solved inside a mix of other jobs gives the same bits."""
+    from hastycompute_b200.toeplitz import System
+    shape = (32, 32, 32)
+    plan = ToeplitzPlan(shape, cuda)
+    jobs = _mixed_jobs(plan, cuda, [7, 8, 9, 10], [4, 8, 2, 6])
+    def solve(sel, graph):
+        xs = {i: torch.zeros(shape, dtype=torch.complex64, device=cuda) for i in sel}
+        plan.cg_systems([System(xs[i], jobs[i]["smt"], jobs[i]["packed"], b=jobs[i]["bt"], coils=jobs[i]["coils"],
+                                lam=jobs[i]["lam"]) for i in sel], iters=6, graph=graph)
+        return xs
+    alone = solve([1], graph=False)[1]
+    mixed = solve([3, 1, 0, 2], graph=True)[1]
+    assert torch.equal(alone, mixed)
