@@ -70,6 +70,9 @@ SIGNATURES = {
                           c_float, c_int, c_double, P_i32, P_i32, c_void_p, c_size, c_void_p]),
     "hb_toeplitz_apply_noalloc": (c_int, [c_i64, c_i64, c_i64, c_void_p, c_void_p, c_i64, c_i64, c_void_p, c_int,
                                           c_void_p, c_void_p]),
+    "hb_autotune_workspace_bytes": (c_size, [c_void_p, c_i64]),
+    "hb_plan_autotune": (c_int, [c_void_p, c_i64, c_void_p, c_size, c_void_p, ctypes.POINTER(c_int),
+                                 ctypes.POINTER(c_double)]),
     "hb_launch_count": (ctypes.c_uint64, []),
     "hb_profile_start": (c_int, []),
     "hb_profile_stop": (c_int, [ctypes.POINTER(c_double), P_i64, c_int]),

@@ -22,6 +22,7 @@ struct hb_plan {
   int device;
   float2* tables;  // device twiddle tables (table_offsets layout)
   TableOffsets to;
+  int plane_variant = -1;  // plane-pass schedule chosen by hb_plan_autotune (-1: default)
 };
 
 namespace {
@@ -206,7 +207,8 @@ cudaError_t launch_b(const PassArgs& a, int nslots, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// Plane-pass variants for the large planes (selected by HB_PLANE_VARIANT for tuning)
+// Plane-pass schedules (cluster split Q x CTA size) per plane size; hb_plan_autotune
+// times them, HB_PLANE_VARIANT overrides, index 0 is the default.
 struct PlaneVariant {
   const char* name;
   PassLauncher fn;
@@ -220,12 +222,30 @@ const PlaneVariant kPlane64[] = {
     {"q1t256", &launch_b<64, 64, 1, 256>}, {"q2t128", &launch_b<64, 64, 2, 128>},
     {"q1t128", &launch_b<64, 64, 1, 128>}, {"q2t256", &launch_b<64, 64, 2, 256>},
 };
+const PlaneVariant kPlane96[] = {
+    {"q1t256", &launch_b<96, 96, 1, 256>}, {"q2t128", &launch_b<96, 96, 2, 128>},
+    {"q2t256", &launch_b<96, 96, 2, 256>},
+};
+const PlaneVariant kPlane160[] = {
+    {"q2t128", &launch_b<160, 160, 2, 128>}, {"q4t128", &launch_b<160, 160, 4, 128>},
+};
 
-int plane_variant_index(int nvariants) {
+const PlaneVariant* plane_variants(int N0, int N1, int* n) {
+  *n = 0;
+  if (N0 == 128 && N1 == 128) { *n = 5; return kPlane128; }
+  if (N0 == 64 && N1 == 64) { *n = 4; return kPlane64; }
+  if (N0 == 96 && N1 == 96) { *n = 3; return kPlane96; }
+  if (N0 == 160 && N1 == 160) { *n = 2; return kPlane160; }
+  return nullptr;
+}
+
+int plane_variant_index(int nvariants, int chosen) {
   const char* env = getenv("HB_PLANE_VARIANT");
-  if (!env) return 0;
-  int v = atoi(env);
-  return (v >= 0 && v < nvariants) ? v : 0;
+  if (env) {
+    int v = atoi(env);
+    return (v >= 0 && v < nvariants) ? v : 0;
+  }
+  return (chosen >= 0 && chosen < nvariants) ? chosen : 0;
 }
 
 // [log2(N2)-3][log2(YT)-3]
@@ -241,12 +261,11 @@ const PassLauncher kLaunchC[7][2] = {HB_XROW(8, launch_c),   HB_XROW(16, launch_
    &launch_b<N0, 128, 1, 512>}
 const PassLauncher kLaunchB[5][5] = {HB_BROW(8), HB_BROW(16), HB_BROW(32), HB_BROW(64), HB_BROW(128)};
 
-PassLauncher plane_launcher(int N0, int N1) {
-  if (N0 == 128 && N1 == 128) return kPlane128[plane_variant_index(5)].fn;
-  if (N0 == 64 && N1 == 64) return kPlane64[plane_variant_index(4)].fn;
-  if (N0 == 96 && N1 == 96) return &launch_b<96, 96, 1, 256>;
-  if (N0 == 160 && N1 == 160) return &launch_b<160, 160, 2, 128>;
-  return kLaunchB[ilog2(N0) - 3][ilog2(N1) - 3];
+PassLauncher plane_launcher(const hb_plan* p) {
+  int n = 0;
+  const PlaneVariant* v = plane_variants(p->N0, p->N1, &n);
+  if (v) return v[plane_variant_index(n, p->plane_variant)].fn;
+  return kLaunchB[ilog2(p->N0) - 3][ilog2(p->N1) - 3];
 }
 
 int yt_for(int N1) { return N1 < 16 ? N1 : 16; }
@@ -259,7 +278,7 @@ int run_normal(const hb_plan* p, PassArgs a, cudaStream_t st) {
   if (nslots > 65535) return fail(HB_ERR_INVALID, "too many system x coil slots in one launch (max 65535)");
   cudaError_t e = kLaunchA[ia][iy](a, nslots, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass A: ") + cudaGetErrorString(e));
-  e = plane_launcher(p->N0, p->N1)(a, nslots, st);
+  e = plane_launcher(p)(a, nslots, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass B: ") + cudaGetErrorString(e));
   e = kLaunchC[ia][iy](a, a.nsys, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass C: ") + cudaGetErrorString(e));
@@ -458,10 +477,11 @@ struct GraphStream {
   cudaEvent_t e1 = nullptr, e2 = nullptr;
 };
 GraphStream g_graph_streams[64];
-std::mutex g_graph_mu;
+std::mutex g_graph_mu;         // serialises use of the side streams
+std::mutex g_graph_create_mu;  // guards their creation
 
 int graph_stream(int dev, GraphStream** out) {
-  std::lock_guard<std::mutex> lk(g_graph_mu);
+  std::lock_guard<std::mutex> lk(g_graph_create_mu);
   if (dev < 0 || dev >= 64) return fail(HB_ERR_INVALID, "device index");
   GraphStream& gs = g_graph_streams[dev];
   if (!gs.ready) {
@@ -546,18 +566,30 @@ int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int it
       for (int it = 0; it < iters; ++it)
         if (int r = cg_iteration(p, ai, s, ugrid, w.iter, st)) return r;
     } else {
-      // capture one iteration on a side stream, replay it `iters` times
-      int dev = 0;
-      HB_CUDA(cudaGetDevice(&dev));
+      // capture one iteration and replay it `iters` times: on the caller's stream, or,
+      // for the legacy default streams (which cannot be captured), on a per-device side
+      // stream ordered against the caller's stream by events
+      const bool own = st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+      std::unique_lock<std::mutex> side_lock(g_graph_mu, std::defer_lock);
+      cudaStream_t cs = st;
       GraphStream* gs = nullptr;
-      if (int r = graph_stream(dev, &gs)) return r;
-      HB_CUDA(cudaEventRecord(gs->e1, st));
-      HB_CUDA(cudaStreamWaitEvent(gs->s, gs->e1, 0));
+      if (!own) {
+        int dev = 0;
+        HB_CUDA(cudaGetDevice(&dev));
+        if (int r = graph_stream(dev, &gs)) return r;
+        side_lock.lock();
+        cs = gs->s;
+        HB_CUDA(cudaEventRecord(gs->e1, st));
+        HB_CUDA(cudaStreamWaitEvent(cs, gs->e1, 0));
+      }
       cudaGraph_t graph = nullptr;
-      HB_CUDA(cudaStreamBeginCapture(gs->s, cudaStreamCaptureModeThreadLocal));
-      int rc = cg_iteration(p, ai, s, ugrid, w.iter, gs->s);
-      cudaError_t ce = cudaStreamEndCapture(gs->s, &graph);
-      if (rc) return rc;
+      HB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      int rc = cg_iteration(p, ai, s, ugrid, w.iter, cs);
+      cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
       if (ce != cudaSuccess) return fail(HB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
       cudaGraphExec_t exec = nullptr;
       ce = cudaGraphInstantiate(&exec, graph, 0);
@@ -565,10 +597,13 @@ int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int it
         cudaGraphDestroy(graph);
         return fail(HB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
       }
-      for (int it = 0; it < iters && ce == cudaSuccess; ++it) ce = cudaGraphLaunch(exec, gs->s);
+      for (int it = 0; it < iters && ce == cudaSuccess; ++it) ce = cudaGraphLaunch(exec, cs);
       g_launches.fetch_add((uint64_t)kKernelsPerCgIteration * iters, std::memory_order_relaxed);
-      cudaError_t ce2 = cudaEventRecord(gs->e2, gs->s);
-      if (ce2 == cudaSuccess) ce2 = cudaStreamWaitEvent(st, gs->e2, 0);
+      cudaError_t ce2 = cudaSuccess;
+      if (!own) {
+        ce2 = cudaEventRecord(gs->e2, cs);
+        if (ce2 == cudaSuccess) ce2 = cudaStreamWaitEvent(st, gs->e2, 0);
+      }
       cudaGraphExecDestroy(exec);
       cudaGraphDestroy(graph);
       if (ce != cudaSuccess) return fail(HB_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(ce));
@@ -968,6 +1003,76 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
   a.out_ldy = out_ldy;
   a.accumulate = accumulate ? 1 : 0;
   return run_normal(&p, a, st);
+}
+
+size_t hb_autotune_workspace_bytes(const hb_plan* p, int64_t nslots) {
+  if (!p || nslots < 1) return 0;
+  Arena ar(nullptr);
+  carve_group(ar, p, 1, nslots, 0, false);
+  ar.take<float>((size_t)hb_diag_packed_floats(p));
+  return ar.off + 256;
+}
+
+int hb_plan_autotune(hb_plan* p, int64_t nslots, void* ws, size_t ws_bytes, void* stream, int* chosen,
+                     double* best_ms) {
+  if (int r = check_plan(p)) return r;
+  if (nslots < 1 || nslots > 65535) return fail(HB_ERR_INVALID, "hb_plan_autotune: nslots");
+  if (!ws || ws_bytes < hb_autotune_workspace_bytes(p, nslots))
+    return fail(HB_ERR_WORKSPACE, "hb_plan_autotune: workspace too small");
+  DeviceGuard dg(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  int nvar = 0;
+  const PlaneVariant* vars = plane_variants(p->N0, p->N1, &nvar);
+  if (!vars) {  // a single schedule: nothing to choose
+    p->plane_variant = 0;
+    if (chosen) *chosen = 0;
+    if (best_ms) *best_ms = 0.0;
+    return HB_OK;
+  }
+  Arena ar(ws);
+  GroupWs w = carve_group(ar, p, 1, nslots, 0, false);
+  float* diag = ar.take<float>((size_t)hb_diag_packed_floats(p));
+  // one system whose nslots coils all use a unit map; only the plane pass runs, on
+  // zeroed data (its timing does not depend on the values)
+  std::vector<int64_t> coils(nslots, 0);
+  hb_system q{};
+  q.x = w.spill;
+  q.out = w.spill;
+  q.smaps = nullptr;
+  q.coils = coils.data();
+  q.ncoil = nslots;
+  q.packed_diag = diag;
+  if (int r = upload_tables(p, w, &q, 0, 1, false, st)) return r;
+  HB_CUDA(cudaMemsetAsync(w.spill, 0, (size_t)nslots * spill_elems_per_slot(p) * sizeof(float2), st));
+  HB_CUDA(cudaMemsetAsync(diag, 0, (size_t)hb_diag_packed_floats(p) * sizeof(float), st));
+  PassArgs a = group_pass_args(p, w, 1, nslots, false);
+  cudaEvent_t e0, e1;
+  HB_CUDA(cudaEventCreate(&e0));
+  HB_CUDA(cudaEventCreate(&e1));
+  int best = 0;
+  double best_t = 1e300;
+  cudaError_t err = cudaSuccess;
+  for (int v = 0; v < nvar && err == cudaSuccess; ++v) {
+    err = vars[v].fn(a, (int)nslots, st);  // warm-up (and shared-memory opt-in)
+    if (err != cudaSuccess) break;
+    err = cudaEventRecord(e0, st);
+    for (int k = 0; k < 3 && err == cudaSuccess; ++k) err = vars[v].fn(a, (int)nslots, st);
+    if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    if (err == cudaSuccess && ms / 3.0 < best_t) {
+      best_t = ms / 3.0;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return fail(HB_ERR_CUDA, std::string("hb_plan_autotune: ") + cudaGetErrorString(err));
+  p->plane_variant = best;
+  if (chosen) *chosen = best;
+  if (best_ms) *best_ms = best_t;
+  return HB_OK;
 }
 
 uint64_t hb_launch_count(void) { return g_launches.load(); }

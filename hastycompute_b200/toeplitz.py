@@ -97,6 +97,17 @@ class ToeplitzPlan:
             self._ws = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
         return self._ws
 
+    def autotune(self, nslots=16):
+        """Times the plane-pass schedules on nslots (system, coil) slots and keeps the
+        fastest for this plan.  Returns (schedule index, ms per launch)."""
+        nb = self.lib.hb_autotune_workspace_bytes(self._h, int(nslots))
+        ws = torch.empty(int(nb), dtype=torch.uint8, device=self.device)
+        chosen = ctypes.c_int(-1)
+        ms = ctypes.c_double(0.0)
+        capi.check(self.lib.hb_plan_autotune(self._h, int(nslots), _ptr(ws), nb, _stream_ptr(self.device),
+                                             ctypes.byref(chosen), ctypes.byref(ms)))
+        return chosen.value, ms.value
+
     # ---------------------------------------------------------------- diagonal ----
     def build_diagonal(self, coords, want_complex=False):
         """FP64 construction of T from a trajectory coords [3, K] float32 (radians).

@@ -9,6 +9,9 @@
  * `stream` is a cudaStream_t (NULL = legacy default stream).  Every call is
  * asynchronous on `stream` unless documented otherwise.
  *
+ * Calls that take systems (hb_toeplitz_apply, hb_sense_normal_apply*, hb_cg_run*)
+ * synchronise `stream` once per group of systems to upload its descriptor tables.
+ *
  * Every function returns HB_OK (0) or an error code; hb_last_error() gives the
  * message of the last failure on the calling thread.  No function aborts the process
  * or traps on the device.
@@ -160,6 +163,15 @@ int hb_cg_run(const hb_plan* plan, int64_t nsys, void* x, const void* b, const v
               const int64_t* diag_index, float lambda, int iters, double tol,
               int32_t* status_host, int32_t* iters_done_host, void* workspace,
               size_t workspace_bytes, void* stream);
+
+/* Autotuner (no counterpart in the reference, which has one cuFFT call per transform):
+ * times every compiled schedule of the plane pass (cluster split x CTA size) for this
+ * plan's image size on `nslots` (system, coil) slots and keeps the fastest in the plan.
+ * Synchronises `stream`.  chosen / best_ms (nullable) receive the schedule index and its
+ * time per launch.  The environment variable HB_PLANE_VARIANT, when set, overrides. */
+size_t hb_autotune_workspace_bytes(const hb_plan* plan, int64_t nslots);
+int hb_plan_autotune(hb_plan* plan, int64_t nslots, void* workspace, size_t workspace_bytes,
+                     void* stream, int* chosen, double* best_ms);
 
 /* Allocation-free variant of hb_toeplitz_apply.  No counterpart in the reference.
  *

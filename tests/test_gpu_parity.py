@@ -227,7 +227,8 @@ def test_invalid_arguments_raise(cuda):
     assert b"NULL" in lib.hb_last_error()
 
 
-@pytest.mark.parametrize("shape,nvar", [((64, 64, 64), 4), ((128, 128, 128), 5)])
+@pytest.mark.parametrize("shape,nvar", [((64, 64, 64), 4), ((128, 128, 128), 5), ((96, 96, 32), 3),
+                                        ((160, 160, 16), 2)])
 def test_plane_variants_agree(cuda, shape, nvar, monkeypatch):
     """Every plane-pass variant (cluster split Q, CTA size) gives bitwise the same result."""
     plan = ToeplitzPlan(shape, cuda)
@@ -323,3 +324,19 @@ def test_result_same_alone_and_in_the_mix(cuda):
     alone = solve([1], graph=False)[1]
     mixed = solve([3, 1, 0, 2], graph=True)[1]
     assert torch.equal(alone, mixed)
+
+
+def test_autotune_picks_a_schedule_and_keeps_results(cuda):
+    shape = (64, 64, 64)
+    plan = ToeplitzPlan(shape, cuda)
+    coords = synth.kooshball(64, 128)
+    packed = plan.build_diagonal(torch.from_numpy(coords))
+    sm = _c64(synth.coil_maps(2, shape, seed=3), cuda)
+    x = _c64(synth.gaussian_image(shape, seed=4), cuda)
+    before = torch.empty_like(x)
+    plan.sense_normal(x, before, sm, packed)
+    chosen, ms = plan.autotune(nslots=8)
+    assert 0 <= chosen < 4 and ms > 0
+    after = torch.empty_like(x)
+    plan.sense_normal(x, after, sm, packed)
+    assert torch.equal(before, after)
