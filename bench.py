@@ -49,6 +49,13 @@ def parse():
     ap.add_argument("--lam", type=float, default=1e-3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", default="batch", choices=["batch", "uneven", "serve"],
+                    help="batch: the 4D-flow batch (default); uneven: heterogeneous jobs; serve: Poisson arrivals")
+    ap.add_argument("--jobs", type=int, default=64, help="uneven/serve: jobs in the mix (serve: pool size)")
+    ap.add_argument("--max-frames", type=int, default=20)
+    ap.add_argument("--rates", default="1,2,4", help="serve: arrival rates (jobs/s)")
+    ap.add_argument("--duration", type=float, default=30.0, help="serve: seconds of arrivals per rate")
+    ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args()
 
 
@@ -174,11 +181,174 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------- heterogeneous job mixes ------
+MIX_SHAPES = [(96, 96, 96), (128, 128, 128), (160, 160, 128)]
+MIX_COILS = [8, 12, 16, 32]
+
+
+def make_job_mix(a, dev, njobs, plans):
+    """Seeded job mix: image size from MIX_SHAPES, coils from MIX_COILS, 1..max_frames
+    frames (one system per frame), a golden-angle kooshball of 1000-4000 spokes x 256.
+    The job's diagonal is built in FP64 from its trajectory and shared by its frames
+    (solve timing does not depend on the diagonal's values); b is a seeded random image."""
+    from hastycompute_b200 import synth
+    from hastycompute_b200.toeplitz import ToeplitzPlan
+
+    rng = np.random.default_rng(a.seed)
+    g = torch.Generator(device=dev).manual_seed(a.seed)
+    jobs = []
+    for j in range(njobs):
+        shape = MIX_SHAPES[int(rng.integers(len(MIX_SHAPES)))]
+        ncoil = MIX_COILS[int(rng.integers(len(MIX_COILS)))]
+        nframes = int(rng.integers(1, a.max_frames + 1))
+        spokes = int(rng.integers(1000, 4001))
+        if shape not in plans:
+            plans[shape] = ToeplitzPlan(shape, dev)
+        plan = plans[shape]
+        coords = torch.from_numpy(synth.kooshball(spokes, a.samples, frame=j % 7, nframes=7))
+        packed = plan.build_diagonal(coords).unsqueeze(0)
+        sm = synth.coil_maps_torch(ncoil, shape, seed=1000 + j, device=dev)
+        b = torch.randn((nframes,) + shape, dtype=torch.complex64, device=dev, generator=g)
+        jobs.append({"shape": shape, "smaps": sm, "packed": packed, "b": b, "frames": nframes, "coils": ncoil,
+                     "spokes": spokes})
+    return jobs
+
+
+def run_uneven(a, dev):
+    import threading
+
+    from hastycompute_b200 import capi
+    from hastycompute_b200.toeplitz import System
+
+    plans = {}
+    t0 = time.perf_counter()
+    jobs = make_job_mix(a, dev, a.jobs, plans)
+    tuned = {str(k): plans[k].autotune(nslots=32) for k in plans}
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    classes = {k: [j for j in jobs if j["shape"] == k] for k in plans}
+    xs = {k: [torch.zeros_like(j["b"]) for j in classes[k]] for k in classes}
+    ws_cap = int(min(24e9, torch.cuda.mem_get_info(dev)[0] * 0.5 / max(1, len(classes))))
+
+    def systems_of(k):
+        out = []
+        for j, x in zip(classes[k], xs[k]):
+            for f in range(j["frames"]):
+                out.append(System(x[f], j["smaps"], j["packed"][0], b=j["b"][f], lam=a.lam))
+        return out
+
+    sysl = {k: systems_of(k) for k in classes}
+    streams = {k: torch.cuda.Stream(dev) for k in classes}
+
+    def solve(k, errs):
+        try:
+            with torch.cuda.stream(streams[k]):
+                plans[k].cg_systems(sysl[k], iters=a.iters, graph=True, workspace_bytes=ws_cap)
+        except Exception as e:  # noqa: BLE001
+            errs.append(e)
+
+    def one_round():
+        errs = []
+        th = [threading.Thread(target=solve, args=(k, errs)) for k in classes]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        if errs:
+            raise errs[0]
+
+    one_round()  # warm-up (graphs, opt-ins)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(dev.index or 0))
+    clocks.start()
+    launches0 = capi.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s_ in streams.values():
+        s_.wait_event(e0)
+    for _ in range(a.steps):
+        one_round()
+    for s_ in streams.values():
+        torch.cuda.current_stream(dev).wait_stream(s_)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    nsys = sum(len(v) for v in sysl.values())
+    applies = nsys * (a.iters + 1) * a.steps
+    line = {
+        "metric": "CG solves/s (uneven batch)", "value": nsys * a.steps / (ms / 1000.0), "unit": "solves/s",
+        "applies_per_s": applies / (ms / 1000.0), "n_gpus": 1, "steps": a.steps, "warmup": 1,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "dtype": "c64 (fp32)", "data": "synthetic (seeded)",
+        "config": {"workload": f"{a.jobs} jobs, sizes {MIX_SHAPES}, coils {MIX_COILS}, 1-{a.max_frames} frames, "
+                               f"1000-4000 spokes x {a.samples}, {a.iters}-iteration CG, one launch sequence per size "
+                               f"class on its own stream, iterations replayed as CUDA graphs",
+                   "systems": nsys, "jobs_per_size": {str(k): len(v) for k, v in classes.items()},
+                   "autotuned_plane_schedule": tuned},
+        "gpu_launches": capi.launch_count() - launches0, "clocks": clk, "setup_s": setup,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(a, dev):
+    from hastycompute_b200.serve import ReconJob, ReconServer
+
+    plans = {}
+    pool = make_job_mix(a, dev, a.jobs, plans)
+    for k in plans:
+        plans[k].autotune(nslots=32)
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(a.seed + 1)
+    results = []
+    for rate in [float(r) for r in a.rates.split(",")]:
+        server = ReconServer(dev, hbm_budget_bytes=int(torch.cuda.mem_get_info(dev)[0] * 0.6), max_active=4)
+        # warm one job through the path
+        j0 = pool[0]
+        server.submit(ReconJob(j0["shape"], j0["smaps"], j0["packed"], [0] * j0["frames"], j0["b"],
+                               iters=a.iters, lam=a.lam)).result()
+        server._results.clear()
+        t_start = time.perf_counter()
+        t_next = t_start
+        futs = []
+        nsys = 0
+        while t_next - t_start < a.duration:
+            now = time.perf_counter()
+            if now < t_next:
+                time.sleep(t_next - now)
+            j = pool[int(rng.integers(len(pool)))]
+            futs.append(server.submit(ReconJob(j["shape"], j["smaps"], j["packed"], [0] * j["frames"], j["b"],
+                                               iters=a.iters, lam=a.lam)))
+            nsys += j["frames"]
+            t_next += float(rng.exponential(1.0 / rate))
+        for f in futs:
+            f.result()
+        t_end = time.perf_counter()
+        server.close()
+        st = server.stats()
+        results.append({"rate_jobs_per_s": rate, "jobs": st["jobs"], "p50_s": st["p50_s"], "p99_s": st["p99_s"],
+                        "mean_s": st["mean_s"], "max_queue_wait_s": st["max_queue_wait_s"],
+                        "solves_per_s": nsys / (t_end - t_start), "wall_s": t_end - t_start})
+    line = {"metric": "p99 recon latency (served)", "value": max(r["p99_s"] for r in results), "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "c64 (fp32)", "data": "synthetic (seeded)",
+            "config": {"workload": f"Poisson arrivals, job pool of {a.jobs} as in the uneven mix, "
+                                   f"{a.duration:.0f} s per rate, {a.iters}-iteration CG, admission by HBM footprint, "
+                                   f"per-job streams (up to 4 concurrent)"},
+            "per_rate": results}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- GPU arm --------
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.mode != "batch":
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dev = torch.device("cuda", local)
+        (run_uneven if a.mode == "uneven" else run_serve)(a, dev)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -69,3 +69,24 @@ def flow_phantom(shape, nenc, seed=0, noise=1e-3, dtype=np.complex64):
         out[e] = mag * np.exp(1j * np.pi * (g[0] * z + g[1] * y + g[2] * x))
         out[e] += noise * (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) / np.sqrt(2.0)
     return out.astype(dtype)
+
+
+def coil_maps_torch(ncoil, shape, seed=0, device="cuda"):
+    """coil_maps() generated on the device (same construction), for large job pools."""
+    import torch
+
+    g = np.random.default_rng(seed)
+    axes = [torch.linspace(-0.5, 0.5, n + 1, dtype=torch.float64, device=device)[:-1] + 0.5 / n for n in shape]
+    z, y, x = torch.meshgrid(*axes, indexing="ij")
+    maps = torch.empty((ncoil,) + tuple(shape), dtype=torch.complex128, device=device)
+    sigma = 0.3
+    for c in range(ncoil):
+        ang = 2.0 * np.pi * c / ncoil
+        cy, cx = 0.35 * np.sin(ang), 0.35 * np.cos(ang)
+        cz = 0.1 * g.standard_normal()
+        mag = torch.exp(-((z - cz) ** 2 + (y - cy) ** 2 + (x - cx) ** 2) / (2 * sigma * sigma))
+        r = g.standard_normal(4)
+        phase = r[0] * np.pi + 1.5 * (r[1] * z + r[2] * y + r[3] * x)
+        maps[c] = mag * torch.exp(1j * phase)
+    norm = torch.sqrt((maps.abs() ** 2).sum(0))
+    return (maps / norm).to(torch.complex64).contiguous()
