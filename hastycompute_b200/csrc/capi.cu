@@ -191,17 +191,27 @@ cudaError_t launch_b(const PassArgs& a, int nslots, cudaStream_t st) {
   const size_t smem = C::SMEM_F2 * sizeof(float2);
   cudaError_t e = ensure_smem<plane_yz_kernel<N0, N1, Q, THREADS>>(smem);
   if (e != cudaSuccess) return e;
-  dim3 grid(2 * Q, nslots, 2 * a.N2);
-  PassArgs b = a;
-  // one wave of clusters ahead: co-resident clusters = SMs * (CTAs per SM) / (2Q)
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // persistent: as many clusters as can be co-resident (cached per kernel and device)
+  static std::atomic<int> cached[64];
+  int dev = 0;
+  e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int ncl = cached[dev & 63].load();
+  if (ncl <= 0) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * Q, 1, 1);
+    cfg.blockDim = dim3(THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    e = cudaOccupancyMaxActiveClusters(&ncl, plane_yz_kernel<N0, N1, Q, THREADS>, &cfg);
+    if (e != cudaSuccess) return e;
+    if (ncl < 1) ncl = 1;
+    cached[dev & 63].store(ncl);
   }
-  const int per_sm = (int)((227 * 1024) / (smem + 1024));
-  b.prefetch_ahead = getenv("HB_NO_L2_PREFETCH") ? 0 : sms * (per_sm < 1 ? 1 : per_sm) / (2 * Q);
+  const long long nitems = (long long)nslots * 2 * a.N2;
+  if (ncl > nitems) ncl = (int)nitems;
+  if (ncl > 65535) ncl = 65535;
+  dim3 grid(2 * Q, ncl, 1);
+  const PassArgs& b = a;
   LaunchScope ls(HB_KERNEL_PLANE_YZ, st);
   plane_yz_kernel<N0, N1, Q, THREADS><<<grid, THREADS, smem, st>>>(b);
   return cudaGetLastError();

@@ -130,7 +130,6 @@ struct PassArgs {
   long long out_ldz, out_ldy;      // element strides of every output image
   int accumulate;                  // 1: out += result, 0: out = result
   double* dot_partials;            // [nsys][nblocks_c] Re<x, out> partials (nullable)
-  int prefetch_ahead;              // plane pass: L2-prefetch distance in clusters (0 = off)
 };
 
 // ------------------------------------------------------------------------ pass A ----
@@ -207,10 +206,6 @@ plane_yz_kernel(PassArgs a) {
   const int rank = (int)cluster.block_rank();
   const int h = rank / Q;  // ky parity
   const int q = rank % Q;  // owned column / row block
-  const int slot = blockIdx.y;
-  const int kx = blockIdx.z;
-  const int sys = a.slot_sys[slot];
-  if (a.active && !a.active[sys]) return;  // uniform for the whole cluster
   const int M2 = 2 * a.N2;
 
   const TableOffsets to = table_offsets(N0, N1, a.N2);
@@ -221,152 +216,170 @@ plane_yz_kernel(PassArgs a) {
   for (int i = threadIdx.x; i < M0; i += C::THREADS) tw_z[i] = a.tables[to.z + i];
   __syncthreads();
 
-  float2* g = a.spill + ((long long)slot * M2 + kx) * N0 * N1;
-  const float* T = a.sys_diag[sys] + (((long long)kx * 2 + h) * N1) * M0;
   float2* Pr[Q];  // column blocks of this parity, one per cluster rank h*Q + q'
 #pragma unroll
   for (int qq = 0; qq < Q; ++qq) Pr[qq] = cluster.map_shared_rank(P, h * Q + qq);
 
-  if constexpr (Q == 1) {
-    // the whole plane lands in the (row-major, padded) column buffer in one burst
-    for (int i = threadIdx.x; i < N0 * N1; i += C::THREADS) cp_async8(&P[(i / N1) * LDP + (i % N1)], g + i);
-    cp_async_commit();
-  }
-  {
-    // warm L2 with the plane the cluster one wave ahead will read (PREFETCH_AHEAD
-    // clusters later in launch order); a hint only
-    const long long cl = (long long)blockIdx.z * gridDim.y + blockIdx.y + a.prefetch_ahead;
-    if (a.prefetch_ahead > 0 && cl < (long long)gridDim.y * gridDim.z) {
-      const long long s2 = cl % gridDim.y, k2 = cl / gridDim.y;
-      const char* nxt = (const char*)(a.spill + (s2 * M2 + k2) * N0 * N1);
+  // Persistent: cluster c of gridDim.y takes work items c, c + gridDim.y, ...; item i is
+  // (slot = i % nslots, kx = i / nslots), so co-resident clusters share kx (and the
+  // diagonal's kx plane in L2).
+  const long long nitems = (long long)a.nslots * M2;
+  const int ncl = gridDim.y;
+#pragma unroll 1
+  for (long long item = blockIdx.y; item < nitems; item += ncl) {
+    const int slot = (int)(item % a.nslots);
+    const int kx = (int)(item / a.nslots);
+    const int sys = a.slot_sys[slot];
+    if (a.active && !a.active[sys]) continue;  // uniform for the whole cluster
+    float2* g = a.spill + ((long long)slot * M2 + kx) * N0 * N1;
+    const float* T = a.sys_diag[sys] + (((long long)kx * 2 + h) * N1) * M0;
+
+    // Q == 1: the plane lands in the (row-major, padded) column buffer in row groups of
+    // NTEAMS_R rows (one asynchronous copy group each); the row FFTs of the first group
+    // start while the later groups are still arriving.
+    constexpr int RG = C::NTEAMS_R;
+    constexpr int NGRP = (ZR + RG - 1) / RG;
+    if constexpr (Q == 1) {
+#pragma unroll 1
+      for (int grp = 0; grp < NGRP; ++grp) {
+        const int r0 = grp * RG, nr = (N0 - r0) < RG ? (N0 - r0) : RG;
+        for (int i = threadIdx.x; i < nr * N1; i += C::THREADS)
+          cp_async8(&P[(r0 + i / N1) * LDP + (i % N1)], g + (long long)r0 * N1 + i);
+        cp_async_commit();
+      }
+    }
+    // warm L2 with this cluster's next plane (a hint only)
+    if (item + ncl < nitems) {
+      const long long nx = item + ncl;
+      const char* nxt = (const char*)(a.spill + ((nx % a.nslots) * M2 + nx / a.nslots) * N0 * N1);
       const int bytes = N0 * N1 * (int)sizeof(float2);
       const int per_cta = bytes / (2 * Q);
       for (int off = threadIdx.x * 128; off < per_cta; off += C::THREADS * 128)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt + rank * per_cta + off));
     }
-  }
-  if constexpr (Q == 1) {
-    cp_async_wait<0>();
-    __syncthreads();
-  }
-
-  // stage 1: owned rows, forward N1-point FFT of the parity-h half; each output column
-  // goes to the CTA that owns it
-  {
-    const int team = threadIdx.x / SR, t = threadIdx.x % SR;
-    const int tr = row_of_team<SR, C::NTEAMS_R, ZR>(team);
-    float2* buf = xbuf + team * C::TBUF_R;
-#pragma unroll 1
-    for (int it = 0; it < LPT; ++it) {
-      const int zl = tr + it * C::NTEAMS_R;
-      const int z = q * ZR + (zl < ZR ? zl : 0);
-      float2 v[ER];
-#pragma unroll
-      for (int e = 0; e < ER; ++e) {
-        const int y = din_index<N1>(t, e);
-        float2 val = Q == 1 ? P[z * LDP + y] : g[(long long)z * N1 + y];
-        if (h) val = cmul(val, par[y]);
-        v[e] = val;
-      }
-      team_fft_din_to_dout<N1, -1, false>(v, t, buf, tw_r);
-      if (zl < ZR) {
-#pragma unroll
-        for (int r = 0; r < ER; ++r) {
-          const int ky = dout_index<N1>(t, r);
-          Pr[ky / H][pos(z) * LDP + ky % H] = v[r];
-        }
-      }
-    }
-  }
-  cluster.sync();
-
-  // stage 2: owned columns, M0-point FFT along z (upper half zero), x T, inverse, crop
-  {
-    const int team = threadIdx.x / SZ, t = threadIdx.x % SZ;
-    float2* buf = xbuf + team * C::TBUF_Z;
-    // this lane's z twiddles, reused by every column (registers when they are few)
-    constexpr bool kRegTw = EZ <= 16;
-    float2 twz[kRegTw ? EZ : 1];
-    if constexpr (kRegTw) load_lane_twiddles<M0>(twz, tw_z, t);
-    // the diagonal's columns are fetched one iteration ahead of their use
-    float tnext[EZ];
+    // stage 1: owned rows, forward N1-point FFT of the parity-h half; each output column
+    // goes to the CTA that owns it
     {
-      const int col = team < H ? team : 0;
-      const float* Tc = T + (long long)(q * H + col) * M0;
-#pragma unroll
-      for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tc + dout_index<M0>(t, r));
-    }
-#pragma unroll 1
-    for (int c0 = 0; c0 < H; c0 += C::NTEAMS_Z) {
-      const int col = c0 + team;
-      const bool ok = col < H;
-      const int colc = ok ? col : 0;
-      float tv[EZ];
-#pragma unroll
-      for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
-      if (c0 + C::NTEAMS_Z < H) {
-        const int cn = c0 + C::NTEAMS_Z + team;
-        const float* Tn = T + (long long)(q * H + (cn < H ? cn : 0)) * M0;
-#pragma unroll
-        for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tn + dout_index<M0>(t, r));
-      }
-      float2 v[EZ];
-#pragma unroll
-      for (int e = 0; e < EZ / 2; ++e) v[e] = P[pos(din_index<M0>(t, e)) * LDP + colc];
-      if constexpr (kRegTw) team_fft_din_to_dout_r<M0, -1, true>(v, t, buf, twz);
-      else team_fft_din_to_dout<M0, -1, true>(v, t, buf, tw_z);
-#pragma unroll
-      for (int r = 0; r < EZ; ++r) v[r] = cscale(v[r], tv[r]);
-      if constexpr (kRegTw) team_fft_dout_to_din_r<M0, 1, true>(v, t, buf, twz);
-      else team_fft_dout_to_din<M0, 1, true>(v, t, buf, tw_z);
-      if (ok) {
-#pragma unroll
-        for (int e = 0; e < EZ / 2; ++e) P[pos(din_index<M0>(t, e)) * LDP + col] = v[e];
-      }
-    }
-  }
-  cluster.sync();
-
-  // stage 3: owned rows gathered from the column owners, inverse N1-point FFT along y,
-  // post-twiddle.  Output row zl replaces the Q buffer rows consumed in the same round.
-  {
-    const int team = threadIdx.x / SR, t = threadIdx.x % SR;
-    const int tr = row_of_team<SR, C::NTEAMS_R, ZR>(team);
-    float2* buf = xbuf + team * C::TBUF_R;
-#pragma unroll 1
-    for (int it = 0; it < LPT; ++it) {
-      const int zl = tr + it * C::NTEAMS_R;
-      const int z = q * ZR + (zl < ZR ? zl : 0);
-      float2 v[ER];
-#pragma unroll
-      for (int r = 0; r < ER; ++r) {
-        const int ky = dout_index<N1>(t, r);
-        v[r] = Pr[ky / H][pos(z) * LDP + ky % H];
-      }
-      if constexpr (Q > 1) cluster.sync();  // every CTA has read this round's rows
-      team_fft_dout_to_din<N1, 1, false>(v, t, buf, tw_r);
-      if (zl < ZR) {
-#pragma unroll
+      const int team = threadIdx.x / SR, t = threadIdx.x % SR;
+      const int tr = row_of_team<SR, C::NTEAMS_R, ZR>(team);
+      float2* buf = xbuf + team * C::TBUF_R;
+  #pragma unroll 1
+      for (int it = 0; it < LPT; ++it) {
+        if constexpr (Q == 1) {
+          cp_async_wait_dyn(NGRP - 1 - it);  // group `it` (rows it*RG ...) has landed
+          __syncthreads();
+        }
+        const int zl = tr + it * C::NTEAMS_R;
+        const int z = q * ZR + (zl < ZR ? zl : 0);
+        float2 v[ER];
+  #pragma unroll
         for (int e = 0; e < ER; ++e) {
           const int y = din_index<N1>(t, e);
-          P[zl * GROW + y] = h ? cmulc(v[e], par[y]) : v[e];
+          float2 val = Q == 1 ? P[z * LDP + y] : g[(long long)z * N1 + y];
+          if (h) val = cmul(val, par[y]);
+          v[e] = val;
+        }
+        team_fft_din_to_dout<N1, -1, false>(v, t, buf, tw_r);
+        if (zl < ZR) {
+  #pragma unroll
+          for (int r = 0; r < ER; ++r) {
+            const int ky = dout_index<N1>(t, r);
+            Pr[ky / H][pos(z) * LDP + ky % H] = v[r];
+          }
         }
       }
     }
-  }
-  cluster.sync();
+    cluster.sync();
 
-  // stage 4: sum the two parities; CTA (h, q) writes the h-th half of rows block q
-  {
-    const float2* other = cluster.map_shared_rank(P, (1 - h) * Q + q);
-    constexpr int HALF = ZR / 2;
-    for (int i = threadIdx.x; i < HALF * N1; i += C::THREADS) {
-      const int zl = h * HALF + i / N1, y = i % N1;
-      g[(long long)(q * ZR + zl) * N1 + y] = cadd(P[zl * GROW + y], other[zl * GROW + y]);
+    // stage 2: owned columns, M0-point FFT along z (upper half zero), x T, inverse, crop
+    {
+      const int team = threadIdx.x / SZ, t = threadIdx.x % SZ;
+      float2* buf = xbuf + team * C::TBUF_Z;
+      // this lane's z twiddles, reused by every column (registers when they are few)
+      constexpr bool kRegTw = EZ <= 16;
+      float2 twz[kRegTw ? EZ : 1];
+      if constexpr (kRegTw) load_lane_twiddles<M0>(twz, tw_z, t);
+      // the diagonal's columns are fetched one iteration ahead of their use
+      float tnext[EZ];
+      {
+        const int col = team < H ? team : 0;
+        const float* Tc = T + (long long)(q * H + col) * M0;
+  #pragma unroll
+        for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tc + dout_index<M0>(t, r));
+      }
+  #pragma unroll 1
+      for (int c0 = 0; c0 < H; c0 += C::NTEAMS_Z) {
+        const int col = c0 + team;
+        const bool ok = col < H;
+        const int colc = ok ? col : 0;
+        float tv[EZ];
+  #pragma unroll
+        for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
+        if (c0 + C::NTEAMS_Z < H) {
+          const int cn = c0 + C::NTEAMS_Z + team;
+          const float* Tn = T + (long long)(q * H + (cn < H ? cn : 0)) * M0;
+  #pragma unroll
+          for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tn + dout_index<M0>(t, r));
+        }
+        float2 v[EZ];
+  #pragma unroll
+        for (int e = 0; e < EZ / 2; ++e) v[e] = P[pos(din_index<M0>(t, e)) * LDP + colc];
+        if constexpr (kRegTw) team_fft_din_to_dout_r<M0, -1, true>(v, t, buf, twz);
+        else team_fft_din_to_dout<M0, -1, true>(v, t, buf, tw_z);
+  #pragma unroll
+        for (int r = 0; r < EZ; ++r) v[r] = cscale(v[r], tv[r]);
+        if constexpr (kRegTw) team_fft_dout_to_din_r<M0, 1, true>(v, t, buf, twz);
+        else team_fft_dout_to_din<M0, 1, true>(v, t, buf, tw_z);
+        if (ok) {
+  #pragma unroll
+          for (int e = 0; e < EZ / 2; ++e) P[pos(din_index<M0>(t, e)) * LDP + col] = v[e];
+        }
+      }
     }
+    cluster.sync();
+
+    // stage 3: owned rows gathered from the column owners, inverse N1-point FFT along y,
+    // post-twiddle.  Output row zl replaces the Q buffer rows consumed in the same round.
+    {
+      const int team = threadIdx.x / SR, t = threadIdx.x % SR;
+      const int tr = row_of_team<SR, C::NTEAMS_R, ZR>(team);
+      float2* buf = xbuf + team * C::TBUF_R;
+  #pragma unroll 1
+      for (int it = 0; it < LPT; ++it) {
+        const int zl = tr + it * C::NTEAMS_R;
+        const int z = q * ZR + (zl < ZR ? zl : 0);
+        float2 v[ER];
+  #pragma unroll
+        for (int r = 0; r < ER; ++r) {
+          const int ky = dout_index<N1>(t, r);
+          v[r] = Pr[ky / H][pos(z) * LDP + ky % H];
+        }
+        if constexpr (Q > 1) cluster.sync();  // every CTA has read this round's rows
+        team_fft_dout_to_din<N1, 1, false>(v, t, buf, tw_r);
+        if (zl < ZR) {
+  #pragma unroll
+          for (int e = 0; e < ER; ++e) {
+            const int y = din_index<N1>(t, e);
+            P[zl * GROW + y] = h ? cmulc(v[e], par[y]) : v[e];
+          }
+        }
+      }
+    }
+    cluster.sync();
+
+    // stage 4: sum the two parities; CTA (h, q) writes the h-th half of rows block q
+    {
+      const float2* other = cluster.map_shared_rank(P, (1 - h) * Q + q);
+      constexpr int HALF = ZR / 2;
+      for (int i = threadIdx.x; i < HALF * N1; i += C::THREADS) {
+        const int zl = h * HALF + i / N1, y = i % N1;
+        g[(long long)(q * ZR + zl) * N1 + y] = cadd(P[zl * GROW + y], other[zl * GROW + y]);
+      }
+    }
+
+    // the partners have read this CTA's buffer before the next item overwrites it
+    cluster.sync();
   }
-  // keep this CTA's shared memory alive until the partners have read it
-  cluster.sync();
 }
 
 // ------------------------------------------------------------------------ pass C ----
