@@ -94,8 +94,10 @@ struct PlaneCfg {
 //   [M2, M2+N1)            team table for L = N1
 //   [M2+N1, M2+N1+M0)      team table for L = M0
 //   [.., +N1)              parity twiddle exp(-2*pi*i*y/M1), y < N1
+//   [.., +N1/2)            team table for L = N1/2 (power-of-two N1 only)
+//   [.., +2*N1)            full circle exp(-2*pi*i*k/M1), k < M1
 struct TableOffsets {
-  int x, row, z, par, total;
+  int x, row, z, par, row2, circ, total;
 };
 __host__ __device__ inline TableOffsets table_offsets(int N0, int N1, int N2) {
   TableOffsets o;
@@ -103,7 +105,9 @@ __host__ __device__ inline TableOffsets table_offsets(int N0, int N1, int N2) {
   o.row = 2 * N2;
   o.z = o.row + N1;
   o.par = o.z + 2 * N0;
-  o.total = o.par + N1;
+  o.row2 = o.par + N1;
+  o.circ = o.row2 + N1 / 2;
+  o.total = o.circ + 2 * N1;
   return o;
 }
 
@@ -130,6 +134,7 @@ struct PassArgs {
   long long out_ldz, out_ldy;      // element strides of every output image
   int accumulate;                  // 1: out += result, 0: out = result
   double* dot_partials;            // [nsys][nblocks_c] Re<x, out> partials (nullable)
+  int prefetch_ahead;              // mod-4 plane pass: L2-prefetch distance in clusters (0 = off)
 };
 
 // ------------------------------------------------------------------------ pass A ----
@@ -380,6 +385,201 @@ plane_yz_kernel(PassArgs a) {
     // the partners have read this CTA's buffer before the next item overwrites it
     cluster.sync();
   }
+}
+
+// ---------------------------------------------------------------- pass B (mod 4) ----
+// Plane pass split four ways: a cluster of 4 CTAs owns one (z, y) plane, CTA q takes the
+// 2x y-grid frequencies ky = 4*ky'' + q.  Its row transform is a pre-twiddle by
+// w_M1^(y*q), a fold y -> y mod N1/2 and an N1/2-point FFT; its z stage runs on N1/2
+// columns; its inverse rows are N1/2-point inverse FFTs R_q.  Only the final sum
+//   out[z][y] = sum_q w_M1^(-y*q) * R_q[z][y mod N1/2]
+// crosses CTAs (distributed shared memory).  A CTA holds a quarter plane (N0 x N1/2),
+// small enough for two CTAs per SM, so one CTA's memory phases overlap another's math.
+template <int N0, int N1, int THREADS_>
+struct PlaneQ4Cfg {
+  static constexpr int M0 = 2 * N0, M1 = 2 * N1, HN = N1 / 2;  // HN: columns / row length
+  static constexpr int THREADS = THREADS_;
+  static constexpr int SR = TeamCfg<HN>::S, ER = TeamCfg<HN>::E;
+  static constexpr int SZ = TeamCfg<M0>::S, EZ = TeamCfg<M0>::E;
+  static constexpr int NTEAMS_R = THREADS / SR, NTEAMS_Z = THREADS / SZ;
+  static constexpr int LPT = (N0 + NTEAMS_R - 1) / NTEAMS_R;
+  static constexpr int LDP = HN + 1;
+  static constexpr int PBUF = N0 * LDP;
+  static constexpr int TBUF_R = team_buf_stride<HN>(), TBUF_Z = team_buf_stride<M0>();
+  static constexpr int XBUF = (NTEAMS_R * TBUF_R > NTEAMS_Z * TBUF_Z) ? NTEAMS_R * TBUF_R : NTEAMS_Z * TBUF_Z;
+  static constexpr int SMEM_F2 = PBUF + XBUF + HN + M0 + M1;  // + tables: row (HN), z (M0), circle (M1)
+  static_assert(N0 % 4 == 0 && HN >= 8, "four-way plane split");
+  static_assert(THREADS % SR == 0 && THREADS % SZ == 0, "teams must tile the CTA");
+};
+
+template <int N0, int N1, int THREADS_>
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(THREADS_)
+plane_q4_kernel(PassArgs a) {
+  namespace cg = cooperative_groups;
+  using C = PlaneQ4Cfg<N0, N1, THREADS_>;
+  constexpr int M0 = C::M0, M1 = C::M1, HN = C::HN, LDP = C::LDP;
+  constexpr int SR = C::SR, ER = C::ER, SZ = C::SZ, EZ = C::EZ;
+  extern __shared__ float2 smem[];
+  float2* P = smem;                 // [N0][LDP]: quarter plane
+  float2* xbuf = P + C::PBUF;
+  float2* tw_r = xbuf + C::XBUF;    // [HN]
+  float2* tw_z = tw_r + HN;         // [M0]
+  float2* circ = tw_z + M0;         // [M1] exp(-2*pi*i*k/M1)
+
+  cg::cluster_group cluster = cg::this_cluster();
+  const int q = (int)cluster.block_rank();  // ky mod 4
+  const int slot = blockIdx.y;
+  const int kx = blockIdx.z;
+  const int sys = a.slot_sys[slot];
+  if (a.active && !a.active[sys]) return;  // uniform for the whole cluster
+  const int M2 = 2 * a.N2;
+
+  const TableOffsets to = table_offsets(N0, N1, a.N2);
+  for (int i = threadIdx.x; i < HN; i += C::THREADS) tw_r[i] = a.tables[to.row2 + i];
+  for (int i = threadIdx.x; i < M0; i += C::THREADS) tw_z[i] = a.tables[to.z + i];
+  for (int i = threadIdx.x; i < M1; i += C::THREADS) circ[i] = a.tables[to.circ + i];
+  __syncthreads();
+
+  float2* g = a.spill + ((long long)slot * M2 + kx) * N0 * N1;
+  {
+    // warm L2 with the plane of the cluster a.prefetch_ahead clusters later (a hint only)
+    const long long cl = (long long)blockIdx.z * gridDim.y + blockIdx.y + a.prefetch_ahead;
+    if (a.prefetch_ahead > 0 && cl < (long long)gridDim.y * gridDim.z) {
+      const char* nxt = (const char*)(a.spill + ((cl % gridDim.y) * M2 + cl / gridDim.y) * N0 * N1);
+      constexpr int per_cta = N0 * N1 * (int)sizeof(float2) / 4;
+      for (int off = threadIdx.x * 128; off < per_cta; off += C::THREADS * 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt + q * per_cta + off));
+    }
+  }
+  // T column of ky = 4*ky'' + q: packed index h = q & 1, ky' = 2*ky'' + (q >> 1)
+  const float* T = a.sys_diag[sys] + (((long long)kx * 2 + (q & 1)) * N1) * M0;
+
+  // stage 1: rows.  Lane t of a row team loads y = t + SR*e (e < 2*ER), twiddles by
+  // w_M1^(y*q), folds y and y + HN, then an HN-point FFT; outputs go to P[z][ky''].
+  {
+    const int team = threadIdx.x / SR, t = threadIdx.x % SR;
+    const int tr = row_of_team<SR, C::NTEAMS_R, N0>(team);
+    float2* buf = xbuf + team * C::TBUF_R;
+    // the next row's values are loaded while the current row is transformed
+    float2 nlo[ER], nhi[ER];
+    {
+      const float2* row = g + (long long)(tr < N0 ? tr : 0) * N1;
+#pragma unroll
+      for (int e = 0; e < ER; ++e) {
+        nlo[e] = row[din_index<HN>(t, e)];
+        nhi[e] = row[din_index<HN>(t, e) + HN];
+      }
+    }
+#pragma unroll 1
+    for (int it = 0; it < C::LPT; ++it) {
+      const int z = tr + it * C::NTEAMS_R;
+      float2 v[ER];
+#pragma unroll
+      for (int e = 0; e < ER; ++e) {
+        const int y0 = din_index<HN>(t, e), y1 = y0 + HN;
+        v[e] = cadd(cmul(nlo[e], circ[(y0 * q) % M1]), cmul(nhi[e], circ[(y1 * q) % M1]));
+      }
+      if (it + 1 < C::LPT) {
+        const int zn = z + C::NTEAMS_R;
+        const float2* row = g + (long long)(zn < N0 ? zn : 0) * N1;
+#pragma unroll
+        for (int e = 0; e < ER; ++e) {
+          nlo[e] = row[din_index<HN>(t, e)];
+          nhi[e] = row[din_index<HN>(t, e) + HN];
+        }
+      }
+      team_fft_din_to_dout<HN, -1, false>(v, t, buf, tw_r);
+      if (z < N0) {
+#pragma unroll
+        for (int r = 0; r < ER; ++r) P[z * LDP + dout_index<HN>(t, r)] = v[r];
+      }
+    }
+  }
+  __syncthreads();
+
+  // stage 2: the quarter's HN columns, M0-point FFT along z (upper half zero), x T,
+  // inverse, crop
+  {
+    const int team = threadIdx.x / SZ, t = threadIdx.x % SZ;
+    float2* buf = xbuf + team * C::TBUF_Z;
+    constexpr bool kRegTw = EZ <= 16;
+    float2 twz[kRegTw ? EZ : 1];
+    if constexpr (kRegTw) load_lane_twiddles<M0>(twz, tw_z, t);
+    auto tcol = [&](int col) { return T + (long long)(2 * col + (q >> 1)) * M0; };
+    float tnext[EZ];
+    {
+      const float* Tc = tcol(team < HN ? team : 0);
+#pragma unroll
+      for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tc + dout_index<M0>(t, r));
+    }
+#pragma unroll 1
+    for (int c0 = 0; c0 < HN; c0 += C::NTEAMS_Z) {
+      const int col = c0 + team;
+      const bool ok = col < HN;
+      const int colc = ok ? col : 0;
+      float tv[EZ];
+#pragma unroll
+      for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
+      if (c0 + C::NTEAMS_Z < HN) {
+        const int cn = c0 + C::NTEAMS_Z + team;
+        const float* Tn = tcol(cn < HN ? cn : 0);
+#pragma unroll
+        for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tn + dout_index<M0>(t, r));
+      }
+      float2 v[EZ];
+#pragma unroll
+      for (int e = 0; e < EZ / 2; ++e) v[e] = P[din_index<M0>(t, e) * LDP + colc];
+      if constexpr (kRegTw) team_fft_din_to_dout_r<M0, -1, true>(v, t, buf, twz);
+      else team_fft_din_to_dout<M0, -1, true>(v, t, buf, tw_z);
+#pragma unroll
+      for (int r = 0; r < EZ; ++r) v[r] = cscale(v[r], tv[r]);
+      if constexpr (kRegTw) team_fft_dout_to_din_r<M0, 1, true>(v, t, buf, twz);
+      else team_fft_dout_to_din<M0, 1, true>(v, t, buf, tw_z);
+      if (ok) {
+#pragma unroll
+        for (int e = 0; e < EZ / 2; ++e) P[din_index<M0>(t, e) * LDP + col] = v[e];
+      }
+    }
+  }
+  __syncthreads();
+
+  // stage 3: rows, HN-point inverse FFT in place: P[z][y'] = R_q[z][y'] (y' < HN)
+  {
+    const int team = threadIdx.x / SR, t = threadIdx.x % SR;
+    const int tr = row_of_team<SR, C::NTEAMS_R, N0>(team);
+    float2* buf = xbuf + team * C::TBUF_R;
+#pragma unroll 1
+    for (int it = 0; it < C::LPT; ++it) {
+      const int z = tr + it * C::NTEAMS_R;
+      const int zc = z < N0 ? z : 0;
+      float2 v[ER];
+#pragma unroll
+      for (int r = 0; r < ER; ++r) v[r] = P[zc * LDP + dout_index<HN>(t, r)];
+      team_fft_dout_to_din<HN, 1, false>(v, t, buf, tw_r);
+      if (z < N0) {
+#pragma unroll
+        for (int e = 0; e < ER; ++e) P[z * LDP + din_index<HN>(t, e)] = v[e];
+      }
+    }
+  }
+  cluster.sync();  // every quarter's R_q is complete
+
+  // stage 4: CTA q writes rows [q*N0/4, (q+1)*N0/4): sum of the four quarters
+  {
+    const float2* R[4];
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) R[qq] = cluster.map_shared_rank(P, qq);
+    constexpr int ROWS = N0 / 4;
+    for (int i = threadIdx.x; i < ROWS * N1; i += C::THREADS) {
+      const int z = q * ROWS + i / N1, y = i % N1, yp = y % HN;
+      float2 acc = R[0][z * LDP + yp];
+#pragma unroll
+      for (int qq = 1; qq < 4; ++qq) acc = cadd(acc, cmulc(R[qq][z * LDP + yp], circ[(y * qq) % M1]));
+      g[(long long)z * N1 + y] = acc;
+    }
+  }
+  // keep this CTA's shared memory alive until the partners have read it
+  cluster.sync();
 }
 
 // ------------------------------------------------------------------------ pass C ----

@@ -227,24 +227,36 @@ def test_invalid_arguments_raise(cuda):
     assert b"NULL" in lib.hb_last_error()
 
 
-@pytest.mark.parametrize("shape,nvar", [((64, 64, 64), 4), ((128, 128, 128), 5), ((96, 96, 32), 3),
-                                        ((160, 160, 16), 2)])
-def test_plane_variants_agree(cuda, shape, nvar, monkeypatch):
-    """Every plane-pass variant (cluster split Q, CTA size) gives bitwise the same result."""
+# schedule index ranges of one arithmetic family: (first, count) of the parity split,
+# (first, count) of the mod-4 split
+@pytest.mark.parametrize("shape,parity,mod4", [((64, 64, 64), (0, 4), (4, 2)), ((128, 128, 128), (1, 5), (0, 1)),
+                                               ((96, 96, 32), (0, 3), (3, 0)), ((160, 160, 16), (0, 2), (2, 0))])
+def test_plane_variants_agree(cuda, shape, parity, mod4, monkeypatch):
+    """Every plane-pass schedule of the parity split (cluster split Q, CTA size) gives
+    bitwise the same result; the mod-4 split (a different arithmetic decomposition)
+    agrees to FP32 rounding."""
     plan = ToeplitzPlan(shape, cuda)
-    rng = np.random.default_rng(21)
     coords = synth.kooshball(64, 2 * shape[0])
-    packed = plan.build_diagonal(torch.from_numpy(coords))
+    packed, Tg = plan.build_diagonal(torch.from_numpy(coords), want_complex=True)
     sm = _c64(synth.coil_maps(2, shape, seed=3), cuda)
-    x = _c64(synth.gaussian_image(shape, seed=4), cuda)
+    xn = synth.gaussian_image(shape, seed=4)
+    x = _c64(xn, cuda)
+    nvar = max(parity[0] + parity[1], mod4[0] + mod4[1])
     outs = []
     for v in range(nvar):
         monkeypatch.setenv("HB_PLANE_VARIANT", str(v))
         out = torch.empty_like(x)
         plan.sense_normal(x, out, sm, packed)
         outs.append(out)
-    for v in range(1, nvar):
-        assert torch.equal(outs[0], outs[v]), v
+    for fam in (parity, mod4):
+        for v in range(fam[0] + 1, fam[0] + fam[1]):
+            assert torch.equal(outs[fam[0]], outs[v]), v
+    for v in range(nvar):
+        assert O.rel_l2(_np(outs[v]), _np(outs[0])) < 1e-6, v
+    if mod4[1] and shape[0] <= 64:  # the mod-4 split against the FP64 oracle
+        ref = O.sense_normal_toeplitz(xn, synth.coil_maps(2, shape, seed=3), _np(Tg))
+        for v in range(mod4[0], mod4[0] + mod4[1]):
+            assert O.rel_l2(_np(outs[v]), ref) < TOL, v
 
 
 @pytest.mark.parametrize("shape,ncoil", [((96, 96, 96), 3), ((160, 160, 128), 2)])
@@ -336,7 +348,7 @@ def test_autotune_picks_a_schedule_and_keeps_results(cuda):
     before = torch.empty_like(x)
     plan.sense_normal(x, before, sm, packed)
     chosen, ms = plan.autotune(nslots=8)
-    assert 0 <= chosen < 4 and ms > 0
+    assert 0 <= chosen < 6 and ms > 0
     after = torch.empty_like(x)
     plan.sense_normal(x, after, sm, packed)
     assert torch.equal(before, after)
