@@ -477,7 +477,8 @@ plane_q4_kernel(PassArgs a) {
 #pragma unroll
       for (int e = 0; e < ER; ++e) {
         const int y0 = din_index<HN>(t, e), y1 = y0 + HN;
-        v[e] = cadd(cmul(nlo[e], circ[(y0 * q) % M1]), cmul(nhi[e], circ[(y1 * q) % M1]));
+        v[e] = q == 0 ? cadd(nlo[e], nhi[e])
+                      : cadd(cmul(nlo[e], circ[(y0 * q) % M1]), cmul(nhi[e], circ[(y1 * q) % M1]));
       }
       if (it + 1 < C::LPT) {
         const int zn = z + C::NTEAMS_R;
@@ -564,18 +565,24 @@ plane_q4_kernel(PassArgs a) {
   }
   cluster.sync();  // every quarter's R_q is complete
 
-  // stage 4: CTA q writes rows [q*N0/4, (q+1)*N0/4): sum of the four quarters
+  // stage 4: CTA q writes rows [q*N0/4, (q+1)*N0/4): sum of the four quarters.  With
+  // u_q = w_M1^(-y*q) R_q[z][y] (y < HN):  out[z][y] = sum_q u_q and, because
+  // w_M1^(-HN*q) = i^q,  out[z][y + HN] = u_0 + i u_1 - u_2 - i u_3.
   {
     const float2* R[4];
 #pragma unroll
     for (int qq = 0; qq < 4; ++qq) R[qq] = cluster.map_shared_rank(P, qq);
     constexpr int ROWS = N0 / 4;
-    for (int i = threadIdx.x; i < ROWS * N1; i += C::THREADS) {
-      const int z = q * ROWS + i / N1, y = i % N1, yp = y % HN;
-      float2 acc = R[0][z * LDP + yp];
-#pragma unroll
-      for (int qq = 1; qq < 4; ++qq) acc = cadd(acc, cmulc(R[qq][z * LDP + yp], circ[(y * qq) % M1]));
-      g[(long long)z * N1 + y] = acc;
+    for (int i = threadIdx.x; i < ROWS * HN; i += C::THREADS) {
+      const int z = q * ROWS + i / HN, y = i % HN;
+      const float2 u0 = R[0][z * LDP + y];
+      const float2 u1 = cmulc(R[1][z * LDP + y], circ[y % M1]);
+      const float2 u2 = cmulc(R[2][z * LDP + y], circ[(2 * y) % M1]);
+      const float2 u3 = cmulc(R[3][z * LDP + y], circ[(3 * y) % M1]);
+      const float2 s02 = cadd(u0, u2), d02 = csub(u0, u2);
+      const float2 s13 = cadd(u1, u3), d13 = rot90<1>(csub(u1, u3));
+      g[(long long)z * N1 + y] = cadd(s02, s13);
+      g[(long long)z * N1 + y + HN] = cadd(d02, d13);
     }
   }
   // keep this CTA's shared memory alive until the partners have read it
