@@ -217,14 +217,14 @@ cudaError_t launch_b(const PassArgs& a, int nslots, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <int N0, int N1, int THREADS>
-cudaError_t launch_bq4(const PassArgs& a, int nslots, cudaStream_t st) {
-  using C = PlaneQ4Cfg<N0, N1, THREADS>;
+template <int N0, int N1, int K, int THREADS>
+cudaError_t launch_bmod(const PassArgs& a, int nslots, cudaStream_t st) {
+  using C = PlaneModCfg<N0, N1, K, THREADS>;
   const size_t smem = C::SMEM_F2 * sizeof(float2);
-  cudaError_t e = ensure_smem<plane_q4_kernel<N0, N1, THREADS>>(smem);
+  cudaError_t e = ensure_smem<plane_mod_kernel<N0, N1, K, THREADS>>(smem);
   if (e != cudaSuccess) return e;
-  dim3 grid(4, nslots, 2 * a.N2);
-  // one wave of clusters ahead: co-resident clusters = SMs * (CTAs per SM) / 4
+  dim3 grid(K, nslots, 2 * a.N2);
+  // one wave of clusters ahead: as many clusters as can be co-resident
   static std::atomic<int> ahead[64];
   int dev = 0;
   e = cudaGetDevice(&dev);
@@ -232,11 +232,11 @@ cudaError_t launch_bq4(const PassArgs& a, int nslots, cudaStream_t st) {
   int pa = ahead[dev & 63].load();
   if (pa <= 0) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(4, 1, 1);
+    cfg.gridDim = dim3(K, 1, 1);
     cfg.blockDim = dim3(THREADS, 1, 1);
     cfg.dynamicSmemBytes = smem;
     int ncl = 0;
-    e = cudaOccupancyMaxActiveClusters(&ncl, plane_q4_kernel<N0, N1, THREADS>, &cfg);
+    e = cudaOccupancyMaxActiveClusters(&ncl, plane_mod_kernel<N0, N1, K, THREADS>, &cfg);
     if (e != cudaSuccess) return e;
     pa = ncl < 1 ? 1 : ncl;
     ahead[dev & 63].store(pa);
@@ -244,7 +244,7 @@ cudaError_t launch_bq4(const PassArgs& a, int nslots, cudaStream_t st) {
   PassArgs b = a;
   b.prefetch_ahead = getenv("HB_NO_L2_PREFETCH") ? 0 : pa;
   LaunchScope ls(HB_KERNEL_PLANE_YZ, st);
-  plane_q4_kernel<N0, N1, THREADS><<<grid, THREADS, smem, st>>>(b);
+  plane_mod_kernel<N0, N1, K, THREADS><<<grid, THREADS, smem, st>>>(b);
   return cudaGetLastError();
 }
 
@@ -255,15 +255,17 @@ struct PlaneVariant {
   PassLauncher fn;
 };
 const PlaneVariant kPlane128[] = {
-    {"mod4t256", &launch_bq4<128, 128, 256>}, {"q1t512", &launch_b<128, 128, 1, 512>},
-    {"q2t256", &launch_b<128, 128, 2, 256>},  {"q2t128", &launch_b<128, 128, 2, 128>},
-    {"q4t256", &launch_b<128, 128, 4, 256>},  {"q4t128", &launch_b<128, 128, 4, 128>},
-    {"mod4t512", &launch_bq4<128, 128, 512>}, {"mod4t128", &launch_bq4<128, 128, 128>},
+    {"mod4t256", &launch_bmod<128, 128, 4, 256>}, {"q1t512", &launch_b<128, 128, 1, 512>},
+    {"q2t256", &launch_b<128, 128, 2, 256>},      {"q2t128", &launch_b<128, 128, 2, 128>},
+    {"q4t256", &launch_b<128, 128, 4, 256>},      {"q4t128", &launch_b<128, 128, 4, 128>},
+    {"mod4t512", &launch_bmod<128, 128, 4, 512>}, {"mod4t128", &launch_bmod<128, 128, 4, 128>},
+    {"mod8t256", &launch_bmod<128, 128, 8, 256>}, {"mod8t128", &launch_bmod<128, 128, 8, 128>},
 };
 const PlaneVariant kPlane64[] = {
     {"q1t256", &launch_b<64, 64, 1, 256>}, {"q2t128", &launch_b<64, 64, 2, 128>},
     {"q1t128", &launch_b<64, 64, 1, 128>}, {"q2t256", &launch_b<64, 64, 2, 256>},
-    {"mod4t256", &launch_bq4<64, 64, 256>}, {"mod4t128", &launch_bq4<64, 64, 128>},
+    {"mod4t256", &launch_bmod<64, 64, 4, 256>}, {"mod4t128", &launch_bmod<64, 64, 4, 128>},
+    {"mod8t128", &launch_bmod<64, 64, 8, 128>},
 };
 const PlaneVariant kPlane96[] = {
     {"q1t256", &launch_b<96, 96, 1, 256>}, {"q2t128", &launch_b<96, 96, 2, 128>},
@@ -275,8 +277,8 @@ const PlaneVariant kPlane160[] = {
 
 const PlaneVariant* plane_variants(int N0, int N1, int* n) {
   *n = 0;
-  if (N0 == 128 && N1 == 128) { *n = 8; return kPlane128; }
-  if (N0 == 64 && N1 == 64) { *n = 6; return kPlane64; }
+  if (N0 == 128 && N1 == 128) { *n = 10; return kPlane128; }
+  if (N0 == 64 && N1 == 64) { *n = 7; return kPlane64; }
   if (N0 == 96 && N1 == 96) { *n = 3; return kPlane96; }
   if (N0 == 160 && N1 == 160) { *n = 2; return kPlane160; }
   return nullptr;
@@ -740,6 +742,9 @@ void fill_tables(float2* h, int N0, int N1, int N2) {
   if ((N1 & (N1 - 1)) == 0 && N1 >= 16) team_table(to.row2, N1 / 2);
   else
     for (int i = 0; i < N1 / 2; ++i) h[to.row2 + i] = make_float2(1.f, 0.f);
+  if ((N1 & (N1 - 1)) == 0 && N1 >= 32) team_table(to.row4, N1 / 4);
+  else
+    for (int i = 0; i < N1 / 4; ++i) h[to.row4 + i] = make_float2(1.f, 0.f);
   for (int k = 0; k < 2 * N1; ++k) {
     const double a = -2.0 * M_PI * (double)k / (double)(2 * N1);
     h[to.circ + k] = make_float2((float)std::cos(a), (float)std::sin(a));
@@ -749,7 +754,7 @@ void fill_tables(float2* h, int N0, int N1, int N2) {
 // ------------------------------------------------ allocation-free Toeplitz apply ----
 // The spill and the twiddle tables of hb_toeplitz_apply_noalloc live in these arrays;
 // host code reaches them only through cudaGetSymbolAddress (per device).
-constexpr int kNoAllocMaxTables = 2 * 160 + 160 + 2 * 160 + 160 + 80 + 2 * 160;
+constexpr int kNoAllocMaxTables = 2 * 160 + 160 + 2 * 160 + 160 + 80 + 40 + 2 * 160;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[HB_NOALLOC_SCRATCH_BYTES];
 static __device__ __align__(256) float2 g_noalloc_tables[kNoAllocMaxTables];
 constexpr int kNoAllocDescBytes = 512;  // descriptor tables of one system

@@ -95,9 +95,10 @@ struct PlaneCfg {
 //   [M2+N1, M2+N1+M0)      team table for L = M0
 //   [.., +N1)              parity twiddle exp(-2*pi*i*y/M1), y < N1
 //   [.., +N1/2)            team table for L = N1/2 (power-of-two N1 only)
+//   [.., +N1/4)            team table for L = N1/4 (power-of-two N1 only)
 //   [.., +2*N1)            full circle exp(-2*pi*i*k/M1), k < M1
 struct TableOffsets {
-  int x, row, z, par, row2, circ, total;
+  int x, row, z, par, row2, row4, circ, total;
 };
 __host__ __device__ inline TableOffsets table_offsets(int N0, int N1, int N2) {
   TableOffsets o;
@@ -106,7 +107,8 @@ __host__ __device__ inline TableOffsets table_offsets(int N0, int N1, int N2) {
   o.z = o.row + N1;
   o.par = o.z + 2 * N0;
   o.row2 = o.par + N1;
-  o.circ = o.row2 + N1 / 2;
+  o.row4 = o.row2 + N1 / 2;
+  o.circ = o.row4 + N1 / 4;
   o.total = o.circ + 2 * N1;
   return o;
 }
@@ -387,47 +389,71 @@ plane_yz_kernel(PassArgs a) {
   }
 }
 
-// ---------------------------------------------------------------- pass B (mod 4) ----
-// Plane pass split four ways: a cluster of 4 CTAs owns one (z, y) plane, CTA q takes the
-// 2x y-grid frequencies ky = 4*ky'' + q.  Its row transform is a pre-twiddle by
-// w_M1^(y*q), a fold y -> y mod N1/2 and an N1/2-point FFT; its z stage runs on N1/2
-// columns; its inverse rows are N1/2-point inverse FFTs R_q.  Only the final sum
-//   out[z][y] = sum_q w_M1^(-y*q) * R_q[z][y mod N1/2]
-// crosses CTAs (distributed shared memory).  A CTA holds a quarter plane (N0 x N1/2),
-// small enough for two CTAs per SM, so one CTA's memory phases overlap another's math.
-template <int N0, int N1, int THREADS_>
-struct PlaneQ4Cfg {
-  static constexpr int M0 = 2 * N0, M1 = 2 * N1, HN = N1 / 2;  // HN: columns / row length
+// ---------------------------------------------------------------- pass B (mod K) ----
+// Plane pass split K ways (K = 4 or 8): a cluster of K CTAs owns one (z, y) plane and
+// CTA q takes the 2x y-grid frequencies ky = K*k + q (k < L = 2*N1/K).  With
+// y = y' + L*m (m < K/2) the row transform is
+//   X_q[k] = FFT_L( w_M1^(y'*q) * sum_m a[y' + L*m] * e^(-2*pi*i*m*q/K) )[k],
+// the z stage runs on the CTA's L columns, and the inverse rows give R_q = IFFT_L.  The
+// only cross-CTA step is the final sum (distributed shared memory): with
+// u_q = w_M1^(-y'*q) R_q[y'],  out[y' + L*m] = sum_q e^(+2*pi*i*m*q/K) u_q  (m < K/2),
+// a K-point inverse DFT of which half the outputs are kept.  A CTA holds only
+// N0 x L of the plane, so several CTAs share an SM and one CTA's memory phases
+// overlap another's arithmetic.
+template <int N0, int N1, int K, int THREADS_>
+struct PlaneModCfg {
+  static constexpr int M0 = 2 * N0, M1 = 2 * N1, L = M1 / K;
   static constexpr int THREADS = THREADS_;
-  static constexpr int SR = TeamCfg<HN>::S, ER = TeamCfg<HN>::E;
+  static constexpr int SR = TeamCfg<L>::S, ER = TeamCfg<L>::E;
   static constexpr int SZ = TeamCfg<M0>::S, EZ = TeamCfg<M0>::E;
   static constexpr int NTEAMS_R = THREADS / SR, NTEAMS_Z = THREADS / SZ;
   static constexpr int LPT = (N0 + NTEAMS_R - 1) / NTEAMS_R;
-  static constexpr int LDP = HN + 1;
+  static constexpr int LDP = L + 1;
   static constexpr int PBUF = N0 * LDP;
-  static constexpr int TBUF_R = team_buf_stride<HN>(), TBUF_Z = team_buf_stride<M0>();
+  static constexpr int TBUF_R = team_buf_stride<L>(), TBUF_Z = team_buf_stride<M0>();
   static constexpr int XBUF = (NTEAMS_R * TBUF_R > NTEAMS_Z * TBUF_Z) ? NTEAMS_R * TBUF_R : NTEAMS_Z * TBUF_Z;
-  static constexpr int SMEM_F2 = PBUF + XBUF + HN + M0 + M1;  // + tables: row (HN), z (M0), circle (M1)
-  static_assert(N0 % 4 == 0 && HN >= 8, "four-way plane split");
+  static constexpr int SMEM_F2 = PBUF + XBUF + L + M0 + M1;  // + tables: row (L), z (M0), circle (M1)
+  static_assert((K == 4 || K == 8) && N0 % K == 0 && L >= 8, "K-way plane split");
   static_assert(THREADS % SR == 0 && THREADS % SZ == 0, "teams must tile the CTA");
 };
 
-template <int N0, int N1, int THREADS_>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(THREADS_)
-plane_q4_kernel(PassArgs a) {
+// v * exp(DIR * 2*pi*i * p / K) for a runtime p (K = 4 or 8): rotations and one
+// multiply by sqrt(1/2) at most
+template <int K, int DIR>
+HB_DEV float2 rootK(float2 v, int p) {
+  p &= K - 1;
+  if constexpr (K == 8) {
+    if (p & 1) {
+      const float2 r = make_float2(kC8 * (v.x - DIR * v.y), kC8 * (v.y + DIR * v.x));  // v * e^(DIR i pi/4)
+      v = r;
+    }
+    p >>= 1;
+  }
+  switch (p & 3) {
+    case 1: return rot90<DIR>(v);
+    case 2: return make_float2(-v.x, -v.y);
+    case 3: return rot90<-DIR>(v);
+    default: return v;
+  }
+}
+
+template <int N0, int N1, int K, int THREADS_>
+__global__ void __cluster_dims__(K, 1, 1) __launch_bounds__(THREADS_)
+plane_mod_kernel(PassArgs a) {
   namespace cg = cooperative_groups;
-  using C = PlaneQ4Cfg<N0, N1, THREADS_>;
-  constexpr int M0 = C::M0, M1 = C::M1, HN = C::HN, LDP = C::LDP;
+  using C = PlaneModCfg<N0, N1, K, THREADS_>;
+  constexpr int M0 = C::M0, M1 = C::M1, L = C::L, LDP = C::LDP;
   constexpr int SR = C::SR, ER = C::ER, SZ = C::SZ, EZ = C::EZ;
+  constexpr int NM = K / 2;  // fold terms per output
   extern __shared__ float2 smem[];
-  float2* P = smem;                 // [N0][LDP]: quarter plane
+  float2* P = smem;                 // [N0][LDP]: this CTA's share of the plane
   float2* xbuf = P + C::PBUF;
-  float2* tw_r = xbuf + C::XBUF;    // [HN]
-  float2* tw_z = tw_r + HN;         // [M0]
+  float2* tw_r = xbuf + C::XBUF;    // [L]
+  float2* tw_z = tw_r + L;          // [M0]
   float2* circ = tw_z + M0;         // [M1] exp(-2*pi*i*k/M1)
 
   cg::cluster_group cluster = cg::this_cluster();
-  const int q = (int)cluster.block_rank();  // ky mod 4
+  const int q = (int)cluster.block_rank();  // ky mod K
   const int slot = blockIdx.y;
   const int kx = blockIdx.z;
   const int sys = a.slot_sys[slot];
@@ -435,7 +461,8 @@ plane_q4_kernel(PassArgs a) {
   const int M2 = 2 * a.N2;
 
   const TableOffsets to = table_offsets(N0, N1, a.N2);
-  for (int i = threadIdx.x; i < HN; i += C::THREADS) tw_r[i] = a.tables[to.row2 + i];
+  const int trow = K == 4 ? to.row2 : to.row4;
+  for (int i = threadIdx.x; i < L; i += C::THREADS) tw_r[i] = a.tables[trow + i];
   for (int i = threadIdx.x; i < M0; i += C::THREADS) tw_z[i] = a.tables[to.z + i];
   for (int i = threadIdx.x; i < M1; i += C::THREADS) circ[i] = a.tables[to.circ + i];
   __syncthreads();
@@ -446,29 +473,27 @@ plane_q4_kernel(PassArgs a) {
     const long long cl = (long long)blockIdx.z * gridDim.y + blockIdx.y + a.prefetch_ahead;
     if (a.prefetch_ahead > 0 && cl < (long long)gridDim.y * gridDim.z) {
       const char* nxt = (const char*)(a.spill + ((cl % gridDim.y) * M2 + cl / gridDim.y) * N0 * N1);
-      constexpr int per_cta = N0 * N1 * (int)sizeof(float2) / 4;
+      constexpr int per_cta = N0 * N1 * (int)sizeof(float2) / K;
       for (int off = threadIdx.x * 128; off < per_cta; off += C::THREADS * 128)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt + q * per_cta + off));
     }
   }
-  // T column of ky = 4*ky'' + q: packed index h = q & 1, ky' = 2*ky'' + (q >> 1)
+  // T column of ky = K*k + q: packed index h = q & 1, ky' = (K/2)*k + (q >> 1)
   const float* T = a.sys_diag[sys] + (((long long)kx * 2 + (q & 1)) * N1) * M0;
 
-  // stage 1: rows.  Lane t of a row team loads y = t + SR*e (e < 2*ER), twiddles by
-  // w_M1^(y*q), folds y and y + HN, then an HN-point FFT; outputs go to P[z][ky''].
+  // stage 1: rows.  Lane t of a row team loads y' + L*m for y' = t + SR*e, folds with
+  // the K-th roots of unity, twiddles once by w_M1^(y'*q), then an L-point FFT.
   {
     const int team = threadIdx.x / SR, t = threadIdx.x % SR;
     const int tr = row_of_team<SR, C::NTEAMS_R, N0>(team);
     float2* buf = xbuf + team * C::TBUF_R;
-    // the next row's values are loaded while the current row is transformed
-    float2 nlo[ER], nhi[ER];
+    float2 nv[NM][ER];  // the next row's values, loaded while the current one is transformed
     {
       const float2* row = g + (long long)(tr < N0 ? tr : 0) * N1;
 #pragma unroll
-      for (int e = 0; e < ER; ++e) {
-        nlo[e] = row[din_index<HN>(t, e)];
-        nhi[e] = row[din_index<HN>(t, e) + HN];
-      }
+      for (int m = 0; m < NM; ++m)
+#pragma unroll
+        for (int e = 0; e < ER; ++e) nv[m][e] = row[din_index<L>(t, e) + L * m];
     }
 #pragma unroll 1
     for (int it = 0; it < C::LPT; ++it) {
@@ -476,29 +501,29 @@ plane_q4_kernel(PassArgs a) {
       float2 v[ER];
 #pragma unroll
       for (int e = 0; e < ER; ++e) {
-        const int y0 = din_index<HN>(t, e), y1 = y0 + HN;
-        v[e] = q == 0 ? cadd(nlo[e], nhi[e])
-                      : cadd(cmul(nlo[e], circ[(y0 * q) % M1]), cmul(nhi[e], circ[(y1 * q) % M1]));
+        float2 acc = nv[0][e];
+#pragma unroll
+        for (int m = 1; m < NM; ++m) acc = cadd(acc, rootK<K, -1>(nv[m][e], m * q));
+        v[e] = q == 0 ? acc : cmul(acc, circ[(din_index<L>(t, e) * q) % M1]);
       }
       if (it + 1 < C::LPT) {
         const int zn = z + C::NTEAMS_R;
         const float2* row = g + (long long)(zn < N0 ? zn : 0) * N1;
 #pragma unroll
-        for (int e = 0; e < ER; ++e) {
-          nlo[e] = row[din_index<HN>(t, e)];
-          nhi[e] = row[din_index<HN>(t, e) + HN];
-        }
+        for (int m = 0; m < NM; ++m)
+#pragma unroll
+          for (int e = 0; e < ER; ++e) nv[m][e] = row[din_index<L>(t, e) + L * m];
       }
-      team_fft_din_to_dout<HN, -1, false>(v, t, buf, tw_r);
+      team_fft_din_to_dout<L, -1, false>(v, t, buf, tw_r);
       if (z < N0) {
 #pragma unroll
-        for (int r = 0; r < ER; ++r) P[z * LDP + dout_index<HN>(t, r)] = v[r];
+        for (int r = 0; r < ER; ++r) P[z * LDP + dout_index<L>(t, r)] = v[r];
       }
     }
   }
   __syncthreads();
 
-  // stage 2: the quarter's HN columns, M0-point FFT along z (upper half zero), x T,
+  // stage 2: the CTA's L columns, M0-point FFT along z (upper half zero), x T,
   // inverse, crop
   {
     const int team = threadIdx.x / SZ, t = threadIdx.x % SZ;
@@ -506,24 +531,24 @@ plane_q4_kernel(PassArgs a) {
     constexpr bool kRegTw = EZ <= 16;
     float2 twz[kRegTw ? EZ : 1];
     if constexpr (kRegTw) load_lane_twiddles<M0>(twz, tw_z, t);
-    auto tcol = [&](int col) { return T + (long long)(2 * col + (q >> 1)) * M0; };
+    auto tcol = [&](int col) { return T + (long long)((K / 2) * col + (q >> 1)) * M0; };
     float tnext[EZ];
     {
-      const float* Tc = tcol(team < HN ? team : 0);
+      const float* Tc = tcol(team < L ? team : 0);
 #pragma unroll
       for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tc + dout_index<M0>(t, r));
     }
 #pragma unroll 1
-    for (int c0 = 0; c0 < HN; c0 += C::NTEAMS_Z) {
+    for (int c0 = 0; c0 < L; c0 += C::NTEAMS_Z) {
       const int col = c0 + team;
-      const bool ok = col < HN;
+      const bool ok = col < L;
       const int colc = ok ? col : 0;
       float tv[EZ];
 #pragma unroll
       for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
-      if (c0 + C::NTEAMS_Z < HN) {
+      if (c0 + C::NTEAMS_Z < L) {
         const int cn = c0 + C::NTEAMS_Z + team;
-        const float* Tn = tcol(cn < HN ? cn : 0);
+        const float* Tn = tcol(cn < L ? cn : 0);
 #pragma unroll
         for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tn + dout_index<M0>(t, r));
       }
@@ -544,7 +569,7 @@ plane_q4_kernel(PassArgs a) {
   }
   __syncthreads();
 
-  // stage 3: rows, HN-point inverse FFT in place: P[z][y'] = R_q[z][y'] (y' < HN)
+  // stage 3: rows, L-point inverse FFT in place: P[z][y'] = R_q[z][y']
   {
     const int team = threadIdx.x / SR, t = threadIdx.x % SR;
     const int tr = row_of_team<SR, C::NTEAMS_R, N0>(team);
@@ -555,34 +580,32 @@ plane_q4_kernel(PassArgs a) {
       const int zc = z < N0 ? z : 0;
       float2 v[ER];
 #pragma unroll
-      for (int r = 0; r < ER; ++r) v[r] = P[zc * LDP + dout_index<HN>(t, r)];
-      team_fft_dout_to_din<HN, 1, false>(v, t, buf, tw_r);
+      for (int r = 0; r < ER; ++r) v[r] = P[zc * LDP + dout_index<L>(t, r)];
+      team_fft_dout_to_din<L, 1, false>(v, t, buf, tw_r);
       if (z < N0) {
 #pragma unroll
-        for (int e = 0; e < ER; ++e) P[z * LDP + din_index<HN>(t, e)] = v[e];
+        for (int e = 0; e < ER; ++e) P[z * LDP + din_index<L>(t, e)] = v[e];
       }
     }
   }
-  cluster.sync();  // every quarter's R_q is complete
+  cluster.sync();  // every R_q is complete
 
-  // stage 4: CTA q writes rows [q*N0/4, (q+1)*N0/4): sum of the four quarters.  With
-  // u_q = w_M1^(-y*q) R_q[z][y] (y < HN):  out[z][y] = sum_q u_q and, because
-  // w_M1^(-HN*q) = i^q,  out[z][y + HN] = u_0 + i u_1 - u_2 - i u_3.
+  // stage 4: CTA q writes rows [q*N0/K, (q+1)*N0/K): u_q = w_M1^(-y'*q) R_q[y'],
+  // out[y' + L*m] = sum_q e^(2*pi*i*m*q/K) u_q for m < K/2 (a K-point inverse DFT)
   {
-    const float2* R[4];
+    const float2* R[K];
 #pragma unroll
-    for (int qq = 0; qq < 4; ++qq) R[qq] = cluster.map_shared_rank(P, qq);
-    constexpr int ROWS = N0 / 4;
-    for (int i = threadIdx.x; i < ROWS * HN; i += C::THREADS) {
-      const int z = q * ROWS + i / HN, y = i % HN;
-      const float2 u0 = R[0][z * LDP + y];
-      const float2 u1 = cmulc(R[1][z * LDP + y], circ[y % M1]);
-      const float2 u2 = cmulc(R[2][z * LDP + y], circ[(2 * y) % M1]);
-      const float2 u3 = cmulc(R[3][z * LDP + y], circ[(3 * y) % M1]);
-      const float2 s02 = cadd(u0, u2), d02 = csub(u0, u2);
-      const float2 s13 = cadd(u1, u3), d13 = rot90<1>(csub(u1, u3));
-      g[(long long)z * N1 + y] = cadd(s02, s13);
-      g[(long long)z * N1 + y + HN] = cadd(d02, d13);
+    for (int qq = 0; qq < K; ++qq) R[qq] = cluster.map_shared_rank(P, qq);
+    constexpr int ROWS = N0 / K;
+    for (int i = threadIdx.x; i < ROWS * L; i += C::THREADS) {
+      const int z = q * ROWS + i / L, y = i % L;
+      float2 u[K];
+      u[0] = R[0][z * LDP + y];
+#pragma unroll
+      for (int qq = 1; qq < K; ++qq) u[qq] = cmulc(R[qq][z * LDP + y], circ[(y * qq) % M1]);
+      Dft<K, 1>::run(u);
+#pragma unroll
+      for (int m = 0; m < NM; ++m) g[(long long)z * N1 + y + L * m] = u[m];
     }
   }
   // keep this CTA's shared memory alive until the partners have read it

@@ -227,36 +227,37 @@ def test_invalid_arguments_raise(cuda):
     assert b"NULL" in lib.hb_last_error()
 
 
-# schedule index ranges of one arithmetic family: (first, count) of the parity split,
-# (first, count) of the mod-4 split
-@pytest.mark.parametrize("shape,parity,mod4", [((64, 64, 64), (0, 4), (4, 2)), ((128, 128, 128), (1, 5), (0, 1)),
-                                               ((96, 96, 32), (0, 3), (3, 0)), ((160, 160, 16), (0, 2), (2, 0))])
-def test_plane_variants_agree(cuda, shape, parity, mod4, monkeypatch):
-    """Every plane-pass schedule of the parity split (cluster split Q, CTA size) gives
-    bitwise the same result; the mod-4 split (a different arithmetic decomposition)
-    agrees to FP32 rounding."""
+# plane-pass schedule indices grouped by arithmetic family: the parity split (cluster
+# split Q x CTA size), the mod-4 split and the mod-8 split (CTA sizes)
+@pytest.mark.parametrize("shape,families", [((64, 64, 64), [[0, 1, 2, 3], [4, 5], [6]]),
+                                            ((128, 128, 128), [[1, 2, 3, 4, 5], [0, 6, 7], [8, 9]]),
+                                            ((96, 96, 32), [[0, 1, 2]]), ((160, 160, 16), [[0, 1]])])
+def test_plane_variants_agree(cuda, shape, families, monkeypatch):
+    """Every schedule of one family gives bitwise the same result; the families differ
+    only by FP32 rounding, and the mod-K splits match the FP64 oracle."""
     plan = ToeplitzPlan(shape, cuda)
     coords = synth.kooshball(64, 2 * shape[0])
     packed, Tg = plan.build_diagonal(torch.from_numpy(coords), want_complex=True)
     sm = _c64(synth.coil_maps(2, shape, seed=3), cuda)
     xn = synth.gaussian_image(shape, seed=4)
     x = _c64(xn, cuda)
-    nvar = max(parity[0] + parity[1], mod4[0] + mod4[1])
-    outs = []
-    for v in range(nvar):
-        monkeypatch.setenv("HB_PLANE_VARIANT", str(v))
-        out = torch.empty_like(x)
-        plan.sense_normal(x, out, sm, packed)
-        outs.append(out)
-    for fam in (parity, mod4):
-        for v in range(fam[0] + 1, fam[0] + fam[1]):
+    outs = {}
+    for fam in families:
+        for v in fam:
+            monkeypatch.setenv("HB_PLANE_VARIANT", str(v))
+            out = torch.empty_like(x)
+            plan.sense_normal(x, out, sm, packed)
+            outs[v] = out
+    for fam in families:
+        for v in fam[1:]:
             assert torch.equal(outs[fam[0]], outs[v]), v
-    for v in range(nvar):
-        assert O.rel_l2(_np(outs[v]), _np(outs[0])) < 1e-6, v
-    if mod4[1] and shape[0] <= 64:  # the mod-4 split against the FP64 oracle
+    first = outs[families[0][0]]
+    for v, o in outs.items():
+        assert O.rel_l2(_np(o), _np(first)) < 1e-6, v
+    if shape[0] <= 64:
         ref = O.sense_normal_toeplitz(xn, synth.coil_maps(2, shape, seed=3), _np(Tg))
-        for v in range(mod4[0], mod4[0] + mod4[1]):
-            assert O.rel_l2(_np(outs[v]), ref) < TOL, v
+        for fam in families:
+            assert O.rel_l2(_np(outs[fam[0]]), ref) < TOL, fam
 
 
 @pytest.mark.parametrize("shape,ncoil", [((96, 96, 96), 3), ((160, 160, 128), 2)])
@@ -348,7 +349,7 @@ def test_autotune_picks_a_schedule_and_keeps_results(cuda):
     before = torch.empty_like(x)
     plan.sense_normal(x, before, sm, packed)
     chosen, ms = plan.autotune(nslots=8)
-    assert 0 <= chosen < 6 and ms > 0
+    assert 0 <= chosen < 7 and ms > 0
     after = torch.empty_like(x)
     plan.sense_normal(x, after, sm, packed)
     assert torch.equal(before, after)
