@@ -8,9 +8,18 @@
 
 namespace hb {
 
+// Complex add/subtract as one packed FP32x2 instruction on sm_100 (same IEEE results
+// as two scalar adds).  Packed multiplies are not used: they need the operands
+// broadcast or swapped within the pair, which costs more than the scalar FMAs.
+#if defined(__CUDA_ARCH__)
+HB_DEV float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+HB_DEV float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+HB_DEV float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+#else
 HB_DEV float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 HB_DEV float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 HB_DEV float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+#endif
 HB_DEV float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
