@@ -162,12 +162,12 @@ cudaError_t ensure_smem(size_t bytes) {
 using PassLauncher = cudaError_t (*)(const PassArgs&, int, cudaStream_t);
 
 template <int N2, int YT>
-cudaError_t launch_a(const PassArgs& a, int nslots, cudaStream_t st) {
+cudaError_t launch_a(const PassArgs& a, int nsys, cudaStream_t st) {
   using C = XPassCfg<N2, YT>;
   const size_t smem = C::SMEM_F2 * sizeof(float2);
   cudaError_t e = ensure_smem<expand_fwd_x_kernel<N2, YT>>(smem);
   if (e != cudaSuccess) return e;
-  dim3 grid(a.N1 / YT, a.N0, nslots);
+  dim3 grid(a.N1 / YT, a.N0, nsys);
   LaunchScope ls(HB_KERNEL_EXPAND_FWD_X, st);
   expand_fwd_x_kernel<N2, YT><<<grid, C::THREADS, smem, st>>>(a);
   return cudaGetLastError();
@@ -321,7 +321,7 @@ int run_normal(const hb_plan* p, PassArgs a, cudaStream_t st) {
   const int ia = axis_index(p->N2), iy = ilog2(yt) - 3;
   const int nslots = a.nslots;
   if (nslots > 65535) return fail(HB_ERR_INVALID, "too many system x coil slots in one launch (max 65535)");
-  cudaError_t e = kLaunchA[ia][iy](a, nslots, st);
+  cudaError_t e = kLaunchA[ia][iy](a, a.nsys, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass A: ") + cudaGetErrorString(e));
   e = plane_launcher(p)(a, nslots, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass B: ") + cudaGetErrorString(e));

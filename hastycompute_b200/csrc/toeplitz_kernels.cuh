@@ -3,7 +3,7 @@
 //   out = sum_c conj(S_c) * crop( IFFT_M( T * FFT_M( pad( S_c * x ) ) ) )     (M = 2N)
 //
 // Pass A  expand_fwd_x : per (slot, z, y-tile): S_c * x, zero-pad along x, M2-point FFT,
-//                        written transposed to the spill  spill[slot][kx][z][y].
+//                        written transposed to the spill  spill[slot][z][kx][y].
 // Pass B  plane_yz     : per (slot, kx) a 2-CTA cluster owns one N0 x N1 (z, y) plane of
 //                        the spill.  CTA h takes the ky-parity-h half of the 2x y-grid
 //                        (ky = 2*ky' + h): pre-twiddle, N1-point FFT along y, then per ky'
@@ -27,8 +27,8 @@
 namespace hb {
 
 // ---------------------------------------------------------------- launch geometry ----
-// Pass A / C: a CTA covers YT consecutive y lines of one z plane; every team of S lanes
-// transforms LPT of them.
+// Pass A / C: a CTA covers YT consecutive y lines of one z plane of one system and loops
+// over the system's coils; every team of S lanes transforms LPT of the lines.
 template <int N2, int YT>
 struct XPassCfg {
   static constexpr int M2 = 2 * N2;
@@ -37,11 +37,15 @@ struct XPassCfg {
   static constexpr int LPT = (YT * S > 256) ? (YT * S / 256) : 1;
   static constexpr int THREADS = YT * S / LPT;
   static constexpr int NTEAMS = THREADS / S;
-  static constexpr int TILE_LD = YT + 1;  // padded row of the [kx][y] staging tile
+  static constexpr int TILE_LD = YT + 1;  // padded row of the [kx][y] tile
   static constexpr int TBUF = team_buf_stride<M2>();
-  // float2 slots of dynamic shared memory: pass A stages one [kx][y] tile, pass C
-  // double-buffers the tiles of consecutive coils
-  static constexpr int SMEM_F2 = M2 * TILE_LD + NTEAMS * TBUF + M2;
+  // a [kx][y] tile; the same space serves as the teams' FFT exchange buffers
+  static constexpr int TILE = (M2 * TILE_LD > NTEAMS * TBUF) ? M2 * TILE_LD : NTEAMS * TBUF;
+  static constexpr int SMT = YT * N2;     // one coil's map rows [y][x]
+  // float2 slots of dynamic shared memory: pass A = one tile (also the exchange
+  // buffers) + two coil-map stages; pass C = two tiles + the exchange buffers; each
+  // + the M2-entry twiddle table
+  static constexpr int SMEM_F2 = TILE + 2 * SMT + M2;
   static constexpr int SMEM_F2_C = 2 * M2 * TILE_LD + NTEAMS * TBUF + M2;
   static_assert(THREADS % 32 == 0, "x-pass CTA must be whole warps");
 };
@@ -131,7 +135,7 @@ struct PassArgs {
   const float* const* sys_diag;    // [nsys] packed diagonal [M2][2][N1][M0]
   const float* sys_lambda;         // [nsys] adds lambda * x (nullable = 0)
   const float2* mul;               // [N0][N1][N2] unconjugated multiplier (single system, nullable)
-  float2* spill;                   // [nslots][M2][N0][N1]
+  float2* spill;                   // [nslots][N0][M2][N1], see spill_offset
   const float2* tables;            // twiddle tables, see table_offsets
   long long out_ldz, out_ldy;      // element strides of every output image
   int accumulate;                  // 1: out += result, 0: out = result
@@ -139,57 +143,104 @@ struct PassArgs {
   int prefetch_ahead;              // mod-4 plane pass: L2-prefetch distance in clusters (0 = off)
 };
 
+// Spill layout [slot][z][kx][y]: the [kx][y] tile of one (slot, z) that passes A and C
+// move is one contiguous M2*N1 block, and row z of the (slot, kx) plane that pass B
+// transforms is N1 contiguous values, M2*N1 apart from row z + 1.
+__host__ __device__ inline long long spill_offset(int slot, int z, int kx, int N0, int N1, int M2) {
+  return (((long long)slot * N0 + z) * M2 + kx) * N1;
+}
+
 // ------------------------------------------------------------------------ pass A ----
+// Per (system, z, y-tile): the x lines stay in registers while the coils stream by; coil
+// c + 1's map rows are copied asynchronously while coil c is transformed and stored.
 template <int N2, int YT>
 __global__ void __launch_bounds__(XPassCfg<N2, YT>::THREADS)
 expand_fwd_x_kernel(PassArgs a) {
   using C = XPassCfg<N2, YT>;
-  constexpr int M2 = C::M2, E = C::E, S = C::S;
+  constexpr int M2 = C::M2, E = C::E, S = C::S, LPT = C::LPT;
   extern __shared__ float2 smem[];
-  float2* tile = smem;                          // [M2][TILE_LD]
-  float2* xbuf = tile + M2 * C::TILE_LD;        // teams' exchange buffers
-  float2* tw = xbuf + C::NTEAMS * C::TBUF;      // [M2]
+  float2* tile = smem;                // [M2][TILE_LD] output tile / exchange buffers
+  float2* smt = tile + C::TILE;       // 2 x [YT][N2] coil-map stages
+  float2* tw = smt + 2 * C::SMT;      // [M2]
 
-  const int slot = blockIdx.z;
-  const int sys = a.slot_sys[slot];
+  const int sys = blockIdx.z;
   if (a.active && !a.active[sys]) return;
-  const int coil = a.slot_coil[slot];
   const int z = blockIdx.y;
   const int y0 = blockIdx.x * YT;
   const int N0 = a.N0, N1 = a.N1;
 
   for (int i = threadIdx.x; i < M2; i += C::THREADS) tw[i] = a.tables[i];
-  __syncthreads();
 
   const int team = threadIdx.x / S, t = threadIdx.x % S;
-  float2* buf = xbuf + team * C::TBUF;
+  float2* buf = tile + team * C::TBUF;
   const long long plane = (long long)N1 * N2;
-  const float2* xs = a.sys_x[sys] + (long long)z * plane;
   const float2* sm = a.sys_smaps[sys];
-  const float2* ss = sm ? sm + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
+  const int slot0 = a.sys_slot0[sys], ncoil = a.sys_nslot[sys];
+
+  auto prefetch = [&](int ci) {  // coil ci's map rows [y0, y0 + YT) of plane z
+    const float2* src = sm + ((long long)a.slot_coil[slot0 + ci] * N0 + z) * plane + (long long)y0 * N2;
+    float2* dst = smt + (ci & 1) * C::SMT;
+    for (int i = threadIdx.x; i < C::SMT; i += C::THREADS) cp_async8(dst + i, src + i);
+    cp_async_commit();
+  };
+  if (sm && ncoil > 0) prefetch(0);
+
+  float2 xv[LPT][E / 2];
+  {
+    const float2* xs = a.sys_x[sys] + (long long)z * plane;
+#pragma unroll
+    for (int l = 0; l < LPT; ++l)
+#pragma unroll
+      for (int e = 0; e < E / 2; ++e)
+        xv[l][e] = xs[(long long)(y0 + team + l * C::NTEAMS) * N2 + din_index<M2>(t, e)];
+  }
 
 #pragma unroll 1
-  for (int it = 0; it < C::LPT; ++it) {
-    const int line = team + it * C::NTEAMS;
-    const long long row = (long long)(y0 + line) * N2;
-    float2 v[E];
-#pragma unroll
-    for (int e = 0; e < E / 2; ++e) {
-      const int xi = din_index<M2>(t, e);
-      float2 val = xs[row + xi];
-      if (ss) val = cmul(val, ss[row + xi]);
-      v[e] = val;
+  for (int ci = 0; ci < ncoil; ++ci) {
+    if (sm) {
+      if (ci + 1 < ncoil) {
+        prefetch(ci + 1);
+        cp_async_wait<1>();  // coil ci's rows have landed
+      } else {
+        cp_async_wait<0>();
+      }
     }
-    team_fft_din_to_dout<M2, -1, true>(v, t, buf, tw);
+    __syncthreads();  // coil ci's rows are visible; the previous tile has been stored
+    const float2* mt = smt + (ci & 1) * C::SMT;
+    float2 v[LPT][E];
 #pragma unroll
-    for (int r = 0; r < E; ++r) tile[dout_index<M2>(t, r) * C::TILE_LD + line] = v[r];
+    for (int l = 0; l < LPT; ++l) {
+      const int line = team + l * C::NTEAMS;
+#pragma unroll
+      for (int e = 0; e < E / 2; ++e)
+        v[l][e] = sm ? cmul(xv[l][e], mt[line * N2 + din_index<M2>(t, e)]) : xv[l][e];
+      team_fft_din_to_dout<M2, -1, true>(v[l], t, buf, tw);
+    }
+    __syncthreads();  // every exchange is done: the space becomes the output tile
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) {
+      const int line = team + l * C::NTEAMS;
+#pragma unroll
+      for (int r = 0; r < E; ++r) tile[dout_index<M2>(t, r) * C::TILE_LD + line] = v[l][r];
+    }
+    __syncthreads();
+    float2* dst = a.spill + spill_offset(slot0 + ci, z, 0, N0, N1, M2) + y0;
+    for (int i = threadIdx.x; i < M2 * YT; i += C::THREADS) {
+      const int kx = i / YT, j = i % YT;
+      dst[kx * N1 + j] = tile[kx * C::TILE_LD + j];
+    }
   }
-  __syncthreads();
+}
 
-  float2* dst = a.spill + (long long)slot * M2 * N0 * N1 + (long long)z * N1 + y0;
-  for (int i = threadIdx.x; i < M2 * YT; i += C::THREADS) {
-    const int kx = i / YT, j = i % YT;
-    dst[(long long)kx * N0 * N1 + j] = tile[kx * C::TILE_LD + j];
+// L2 prefetch (a hint) of rows [r0, r0 + nrows) of a spill plane, rows `pitch` apart,
+// N1 values each, in 128-byte lines spread over the CTA's threads
+template <int THREADS>
+__device__ __forceinline__ void prefetch_plane_rows_l2(const float2* plane, long long pitch, int r0, int nrows,
+                                                       int N1) {
+  const int lines = N1 * (int)sizeof(float2) / 128;  // per row
+  for (int i = threadIdx.x; i < nrows * lines; i += THREADS) {
+    const char* p = (const char*)(plane + (long long)(r0 + i / lines) * pitch) + (i % lines) * 128;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
   }
 }
 
@@ -214,6 +265,7 @@ plane_yz_kernel(PassArgs a) {
   const int h = rank / Q;  // ky parity
   const int q = rank % Q;  // owned column / row block
   const int M2 = 2 * a.N2;
+  const long long RS = (long long)M2 * N1;  // spill row pitch of a plane
 
   const TableOffsets to = table_offsets(N0, N1, a.N2);
   for (int i = threadIdx.x; i < N1; i += C::THREADS) {
@@ -238,7 +290,7 @@ plane_yz_kernel(PassArgs a) {
     const int kx = (int)(item / a.nslots);
     const int sys = a.slot_sys[slot];
     if (a.active && !a.active[sys]) continue;  // uniform for the whole cluster
-    float2* g = a.spill + ((long long)slot * M2 + kx) * N0 * N1;
+    float2* g = a.spill + spill_offset(slot, 0, kx, N0, N1, M2);  // row z at g + z * RS
     const float* T = a.sys_diag[sys] + (((long long)kx * 2 + h) * N1) * M0;
 
     // Q == 1: the plane lands in the (row-major, padded) column buffer in row groups of
@@ -251,18 +303,15 @@ plane_yz_kernel(PassArgs a) {
       for (int grp = 0; grp < NGRP; ++grp) {
         const int r0 = grp * RG, nr = (N0 - r0) < RG ? (N0 - r0) : RG;
         for (int i = threadIdx.x; i < nr * N1; i += C::THREADS)
-          cp_async8(&P[(r0 + i / N1) * LDP + (i % N1)], g + (long long)r0 * N1 + i);
+          cp_async8(&P[(r0 + i / N1) * LDP + (i % N1)], g + (long long)(r0 + i / N1) * RS + (i % N1));
         cp_async_commit();
       }
     }
     // warm L2 with this cluster's next plane (a hint only)
     if (item + ncl < nitems) {
       const long long nx = item + ncl;
-      const char* nxt = (const char*)(a.spill + ((nx % a.nslots) * M2 + nx / a.nslots) * N0 * N1);
-      const int bytes = N0 * N1 * (int)sizeof(float2);
-      const int per_cta = bytes / (2 * Q);
-      for (int off = threadIdx.x * 128; off < per_cta; off += C::THREADS * 128)
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt + rank * per_cta + off));
+      const float2* nxt = a.spill + spill_offset((int)(nx % a.nslots), 0, (int)(nx / a.nslots), N0, N1, M2);
+      prefetch_plane_rows_l2<C::THREADS>(nxt, RS, rank * (N0 / (2 * Q)), N0 / (2 * Q), N1);
     }
     // stage 1: owned rows, forward N1-point FFT of the parity-h half; each output column
     // goes to the CTA that owns it
@@ -282,7 +331,7 @@ plane_yz_kernel(PassArgs a) {
   #pragma unroll
         for (int e = 0; e < ER; ++e) {
           const int y = din_index<N1>(t, e);
-          float2 val = Q == 1 ? P[z * LDP + y] : g[(long long)z * N1 + y];
+          float2 val = Q == 1 ? P[z * LDP + y] : g[(long long)z * RS + y];
           if (h) val = cmul(val, par[y]);
           v[e] = val;
         }
@@ -380,7 +429,7 @@ plane_yz_kernel(PassArgs a) {
       constexpr int HALF = ZR / 2;
       for (int i = threadIdx.x; i < HALF * N1; i += C::THREADS) {
         const int zl = h * HALF + i / N1, y = i % N1;
-        g[(long long)(q * ZR + zl) * N1 + y] = cadd(P[zl * GROW + y], other[zl * GROW + y]);
+        g[(long long)(q * ZR + zl) * RS + y] = cadd(P[zl * GROW + y], other[zl * GROW + y]);
       }
     }
 
@@ -467,15 +516,14 @@ plane_mod_kernel(PassArgs a) {
   for (int i = threadIdx.x; i < M1; i += C::THREADS) circ[i] = a.tables[to.circ + i];
   __syncthreads();
 
-  float2* g = a.spill + ((long long)slot * M2 + kx) * N0 * N1;
+  const long long RS = (long long)M2 * N1;  // spill row pitch of a plane
+  float2* g = a.spill + spill_offset(slot, 0, kx, N0, N1, M2);  // row z at g + z * RS
   {
     // warm L2 with the plane of the cluster a.prefetch_ahead clusters later (a hint only)
     const long long cl = (long long)blockIdx.z * gridDim.y + blockIdx.y + a.prefetch_ahead;
     if (a.prefetch_ahead > 0 && cl < (long long)gridDim.y * gridDim.z) {
-      const char* nxt = (const char*)(a.spill + ((cl % gridDim.y) * M2 + cl / gridDim.y) * N0 * N1);
-      constexpr int per_cta = N0 * N1 * (int)sizeof(float2) / K;
-      for (int off = threadIdx.x * 128; off < per_cta; off += C::THREADS * 128)
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(nxt + q * per_cta + off));
+      const float2* nxt = a.spill + spill_offset((int)(cl % gridDim.y), 0, (int)(cl / gridDim.y), N0, N1, M2);
+      prefetch_plane_rows_l2<C::THREADS>(nxt, RS, q * (N0 / K), N0 / K, N1);
     }
   }
   // T column of ky = K*k + q: packed index h = q & 1, ky' = (K/2)*k + (q >> 1)
@@ -489,7 +537,7 @@ plane_mod_kernel(PassArgs a) {
     float2* buf = xbuf + team * C::TBUF_R;
     float2 nv[NM][ER];  // the next row's values, loaded while the current one is transformed
     {
-      const float2* row = g + (long long)(tr < N0 ? tr : 0) * N1;
+      const float2* row = g + (long long)(tr < N0 ? tr : 0) * RS;
 #pragma unroll
       for (int m = 0; m < NM; ++m)
 #pragma unroll
@@ -508,7 +556,7 @@ plane_mod_kernel(PassArgs a) {
       }
       if (it + 1 < C::LPT) {
         const int zn = z + C::NTEAMS_R;
-        const float2* row = g + (long long)(zn < N0 ? zn : 0) * N1;
+        const float2* row = g + (long long)(zn < N0 ? zn : 0) * RS;
 #pragma unroll
         for (int m = 0; m < NM; ++m)
 #pragma unroll
@@ -605,7 +653,7 @@ plane_mod_kernel(PassArgs a) {
       for (int qq = 1; qq < K; ++qq) u[qq] = cmulc(R[qq][z * LDP + y], circ[(y * qq) % M1]);
       Dft<K, 1>::run(u);
 #pragma unroll
-      for (int m = 0; m < NM; ++m) g[(long long)z * N1 + y + L * m] = u[m];
+      for (int m = 0; m < NM; ++m) g[(long long)z * RS + y + L * m] = u[m];
     }
   }
   // keep this CTA's shared memory alive until the partners have read it
@@ -620,7 +668,7 @@ inv_x_combine_kernel(PassArgs a) {
   constexpr int M2 = C::M2, E = C::E, S = C::S, LPT = C::LPT;
   extern __shared__ float2 smem[];
   float2* tiles = smem;                          // 2 x [M2][TILE_LD]
-  float2* xbuf = tiles + 2 * M2 * C::TILE_LD;
+  float2* xbuf = tiles + 2 * M2 * C::TILE_LD;    // teams' exchange buffers
   float2* tw = xbuf + C::NTEAMS * C::TBUF;
   __shared__ double red[32];
 
@@ -635,16 +683,15 @@ inv_x_combine_kernel(PassArgs a) {
   const int team = threadIdx.x / S, t = threadIdx.x % S;
   float2* buf = xbuf + team * C::TBUF;
   const long long plane = (long long)N1 * N2;
-  const long long slot_stride = (long long)M2 * N0 * N1;
 
   const int slot0 = a.sys_slot0[sys], ncoil = a.sys_nslot[sys];
   // asynchronous copy of coil ci's [kx][y] tile into tiles[ci & 1]
   auto prefetch = [&](int ci) {
-    const float2* src = a.spill + (long long)(slot0 + ci) * slot_stride + (long long)z * N1 + y0;
+    const float2* src = a.spill + spill_offset(slot0 + ci, z, 0, N0, N1, M2) + y0;
     float2* dst = tiles + (ci & 1) * M2 * C::TILE_LD;
     for (int i = threadIdx.x; i < M2 * YT; i += C::THREADS) {
       const int kx = i / YT, j = i % YT;
-      cp_async8(&dst[kx * C::TILE_LD + j], src + (long long)kx * N0 * N1 + j);
+      cp_async8(&dst[kx * C::TILE_LD + j], src + kx * N1 + j);
     }
     cp_async_commit();
   };
