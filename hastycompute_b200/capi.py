@@ -73,13 +73,21 @@ SIGNATURES = {
     "hb_autotune_workspace_bytes": (c_size, [c_void_p, c_i64]),
     "hb_plan_autotune": (c_int, [c_void_p, c_i64, c_void_p, c_size, c_void_p, ctypes.POINTER(c_int),
                                  ctypes.POINTER(c_double)]),
+    "hb_nufft_create": (c_int, [ctypes.POINTER(c_void_p), c_i64, c_i64, c_i64, c_void_p, c_i64, c_double, c_int,
+                                c_int, c_void_p]),
+    "hb_nufft_destroy": (c_int, [c_void_p]),
+    "hb_nufft_width": (c_int, [c_void_p]),
+    "hb_nufft_type1": (c_int, [c_void_p, c_void_p, c_void_p, c_i64, c_int, c_void_p]),
+    "hb_nufft_type2": (c_int, [c_void_p, c_void_p, c_void_p, c_i64, c_int, c_void_p]),
+    "hb_sense_adjoint_nufft": (c_int, [c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, c_int, c_void_p]),
+    "hb_sense_forward_nufft": (c_int, [c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, c_void_p]),
     "hb_launch_count": (ctypes.c_uint64, []),
     "hb_profile_start": (c_int, []),
     "hb_profile_stop": (c_int, [ctypes.POINTER(c_double), P_i64, c_int]),
 }
 
-HB_KERNEL_KINDS = 5
-KERNEL_NAMES = ["expand_fwd_x", "plane_yz", "inv_x_combine", "cg_update", "diag"]
+HB_KERNEL_KINDS = 6
+KERNEL_NAMES = ["expand_fwd_x", "plane_yz", "inv_x_combine", "cg_update", "diag", "nufft"]
 
 _lib = None
 

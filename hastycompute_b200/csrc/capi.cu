@@ -13,6 +13,7 @@
 #include "../../include/hasty_b200.h"
 #include "cg_kernels.cuh"
 #include "diag_kernels.cuh"
+#include "runtime.cuh"
 #include "toeplitz_kernels.cuh"
 
 using namespace hb;
@@ -26,27 +27,6 @@ struct hb_plan {
 };
 
 namespace {
-
-thread_local std::string g_err;
-
-int fail(int code, const std::string& msg) {
-  g_err = msg;
-  return code;
-}
-
-#define HB_CUDA(call)                                                                 \
-  do {                                                                                \
-    cudaError_t _e = (call);                                                          \
-    if (_e != cudaSuccess)                                                            \
-      return fail(HB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));   \
-  } while (0)
-
-#define HB_CHECK_LAUNCH()                                                             \
-  do {                                                                                \
-    cudaError_t _e = cudaGetLastError();                                              \
-    if (_e != cudaSuccess)                                                            \
-      return fail(HB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(_e)); \
-  } while (0)
 
 // Supported axis lengths and their row in the launcher tables.
 int axis_index(int64_t n) {
@@ -68,79 +48,6 @@ int ilog2(int n) {
   return l;
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  bool ok = true;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess) { ok = false; return; }
-    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) ok = false;
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-  }
-};
-
-// ------------------------------------------------------------ launch accounting ----
-std::atomic<uint64_t> g_launches{0};
-struct ProfRec {
-  int kind;
-  cudaEvent_t a, b;
-};
-std::mutex g_prof_mu;
-std::atomic<bool> g_prof_on{false};
-std::vector<ProfRec> g_prof;
-std::vector<cudaEvent_t> g_ev_pool;
-
-cudaEvent_t take_event() {
-  std::lock_guard<std::mutex> lk(g_prof_mu);
-  if (!g_ev_pool.empty()) {
-    cudaEvent_t e = g_ev_pool.back();
-    g_ev_pool.pop_back();
-    return e;
-  }
-  cudaEvent_t e = nullptr;
-  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
-  return e;
-}
-
-// Counts one kernel launch; while profiling, brackets it with an event pair on `st`.
-struct LaunchScope {
-  int kind;
-  cudaStream_t st;
-  cudaEvent_t a = nullptr, b = nullptr;
-  LaunchScope(int k, cudaStream_t s) : kind(k), st(s) {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;  // graph replays count
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    if (g_prof_on.load(std::memory_order_relaxed)) {
-      a = take_event();
-      b = take_event();
-      if (a && b) cudaEventRecord(a, st);
-    }
-  }
-  ~LaunchScope() {
-    if (a && b) {
-      cudaEventRecord(b, st);
-      std::lock_guard<std::mutex> lk(g_prof_mu);
-      g_prof.push_back({kind, a, b});
-    }
-  }
-};
-
-// Bump allocator over a caller workspace (dry run when base == nullptr).
-struct Arena {
-  char* base;
-  size_t off = 0;
-  explicit Arena(void* b) : base((char*)b) {}
-  template <typename T>
-  T* take(size_t n) {
-    off = (off + 255) & ~size_t(255);
-    T* p = base ? (T*)(base + off) : nullptr;
-    off += n * sizeof(T);
-    return p;
-  }
-};
 
 // Opt-in to large dynamic shared memory, once per kernel and device (the first call of
 // a kernel on a device happens outside any stream capture).

@@ -1,0 +1,418 @@
+// C ABI of the NUFFT (types 1 and 2) and the SENSE forward/adjoint around it
+// (include/hasty_b200.h, section "Non-uniform FFT").  Replaces the cufinufft plans of
+// hasty::fft::CUDANufft (lib/fft/nufft.cpp:540-767, declared nufft.ixx:108-160) and the
+// coil loops of the SENSE operators that use them (lib/mri/sense.ixx:426-497).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/hasty_b200.h"
+#include "fft3_kernels.cuh"
+#include "nufft_kernels.cuh"
+#include "runtime.cuh"
+
+using namespace hb;
+
+struct hb_nufft {
+  int device;
+  NufftGeom g;
+  int maxbatch;
+  float* coords = nullptr;  // [3][K] (a copy)
+  int* perm = nullptr;      // [K] samples in bin order
+  float* corr = nullptr;    // [N0 | N1 | N2] 1 / phi_hat
+  float2* tw = nullptr;     // team twiddle tables of n0, n1, n2 (offsets 0, n0, n0 + n1)
+  float2* grid = nullptr;   // [maxbatch][n0][n1][n2]
+  float2* modes = nullptr;  // [maxbatch][N0][N1][N2] (SENSE temporaries)
+};
+
+namespace {
+
+bool team_length(int L, int* E, int* S) {
+  switch (L) {
+    case 8: *E = 4; *S = 2; return true;
+    case 16: *E = 4; *S = 4; return true;
+    case 32: *E = 8; *S = 4; return true;
+    case 64: *E = 8; *S = 8; return true;
+    case 128: *E = 16; *S = 8; return true;
+    case 256: *E = 16; *S = 16; return true;
+    case 96: *E = 24; *S = 4; return true;
+    case 160: *E = 40; *S = 4; return true;
+    case 192: *E = 24; *S = 8; return true;
+    case 320: *E = 40; *S = 8; return true;
+    default: return false;
+  }
+}
+
+// Kernel width for a requested tolerance (upsampling 2): w = ceil(log10(1/tol)) + 1.
+int width_for_tol(double tol) {
+  int w = (int)std::ceil(std::log10(1.0 / tol)) + 1;
+  return w < 2 ? 2 : (w > 16 ? 16 : w);
+}
+
+// phi_hat(k) = integral over |z| < w/2 of phi(z) cos(2 pi k z / n), composite Simpson
+// rule in FP64 (phi is smooth inside the support and ~exp(-beta) at its edges).
+double phi_hat(int k, int n, int w, double beta) {
+  const int M = 4000;
+  const double hw = 0.5 * w, h = hw / M;
+  auto f = [&](double z) {
+    const double t = z / hw, s = 1.0 - t * t;
+    const double phi = s > 0.0 ? std::exp(beta * (std::sqrt(s) - 1.0)) : 0.0;
+    return phi * std::cos(2.0 * M_PI * k * z / n);
+  };
+  double acc = f(0.0) + f(hw);
+  for (int i = 1; i < M; ++i) acc += (i & 1 ? 4.0 : 2.0) * f(i * h);
+  return 2.0 * acc * h / 3.0;  // even integrand: twice the half-interval
+}
+
+// ---- 3D FFT of nt grids [n0][n1][n2], in place ----
+template <auto kernel>
+cudaError_t allow_smem(size_t bytes) {
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || done[dev & 63] || bytes <= 48 * 1024) return e;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done[dev & 63] = true;
+  return e;
+}
+
+template <int L, int DIR>
+cudaError_t lines_contig(float2* d, long long nlines, const float2* tw, cudaStream_t st) {
+  using C = LineCfg<L>;
+  const size_t smem = C::SMEM_C * sizeof(float2);
+  cudaError_t e = allow_smem<fft_lines_contig_kernel<L, DIR>>(smem);
+  if (e != cudaSuccess) return e;
+  long long blocks = (nlines + C::NTEAMS_C - 1) / C::NTEAMS_C;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  LaunchScope ls(HB_KERNEL_NUFFT, st);
+  fft_lines_contig_kernel<L, DIR><<<(unsigned)blocks, C::THREADS_C, smem, st>>>(d, nlines, tw);
+  return cudaGetLastError();
+}
+
+template <int L, int DIR>
+cudaError_t lines_strided(float2* d, long long row_stride, int ncols, int ny, long long oy, int nz, long long oz,
+                          const float2* tw, cudaStream_t st) {
+  using C = LineCfg<L>;
+  const size_t smem = C::SMEM_S * sizeof(float2);
+  cudaError_t e = allow_smem<fft_lines_strided_kernel<L, DIR>>(smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((ncols + C::XT - 1) / C::XT, ny, nz);
+  LaunchScope ls(HB_KERNEL_NUFFT, st);
+  fft_lines_strided_kernel<L, DIR><<<grid, C::THREADS_S, smem, st>>>(d, row_stride, ncols, oy, oz, tw);
+  return cudaGetLastError();
+}
+
+template <int DIR>
+cudaError_t contig_any(int L, float2* d, long long nlines, const float2* tw, cudaStream_t st) {
+  switch (L) {
+    case 8: return lines_contig<8, DIR>(d, nlines, tw, st);
+    case 16: return lines_contig<16, DIR>(d, nlines, tw, st);
+    case 32: return lines_contig<32, DIR>(d, nlines, tw, st);
+    case 64: return lines_contig<64, DIR>(d, nlines, tw, st);
+    case 128: return lines_contig<128, DIR>(d, nlines, tw, st);
+    case 256: return lines_contig<256, DIR>(d, nlines, tw, st);
+    case 96: return lines_contig<96, DIR>(d, nlines, tw, st);
+    case 160: return lines_contig<160, DIR>(d, nlines, tw, st);
+    case 192: return lines_contig<192, DIR>(d, nlines, tw, st);
+    case 320: return lines_contig<320, DIR>(d, nlines, tw, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int DIR>
+cudaError_t strided_any(int L, float2* d, long long rs, int ncols, int ny, long long oy, int nz, long long oz,
+                        const float2* tw, cudaStream_t st) {
+  switch (L) {
+    case 8: return lines_strided<8, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 16: return lines_strided<16, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 32: return lines_strided<32, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 64: return lines_strided<64, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 128: return lines_strided<128, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 256: return lines_strided<256, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 96: return lines_strided<96, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 160: return lines_strided<160, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 192: return lines_strided<192, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 320: return lines_strided<320, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int DIR>
+cudaError_t fft3(const hb_nufft* p, float2* grid, int nt, cudaStream_t st) {
+  const int n0 = p->g.n[0], n1 = p->g.n[1], n2 = p->g.n[2];
+  const long long vol = (long long)n0 * n1 * n2;
+  cudaError_t e = contig_any<DIR>(n2, grid, (long long)nt * n0 * n1, p->tw + n0 + n1, st);
+  if (e != cudaSuccess) return e;
+  e = strided_any<DIR>(n1, grid, n2, n2, n0, (long long)n1 * n2, nt, vol, p->tw + n0, st);
+  if (e != cudaSuccess) return e;
+  return strided_any<DIR>(n0, grid, (long long)n1 * n2, n2, n1, n2, nt, vol, p->tw, st);
+}
+
+template <int W>
+cudaError_t spread_w(const hb_nufft* p, const float2* c, long long c_ld, int nb, cudaStream_t st) {
+  dim3 grid((unsigned)((p->g.K + 255) / 256), nb);
+  LaunchScope ls(HB_KERNEL_NUFFT, st);
+  nufft_spread_kernel<W><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, c, c_ld, p->grid);
+  return cudaGetLastError();
+}
+template <int W>
+cudaError_t interp_w(const hb_nufft* p, float2* c, long long c_ld, int nb, cudaStream_t st) {
+  dim3 grid((unsigned)((p->g.K + 255) / 256), nb);
+  LaunchScope ls(HB_KERNEL_NUFFT, st);
+  nufft_interp_kernel<W><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, p->grid, c, c_ld);
+  return cudaGetLastError();
+}
+
+#define HB_W_DISPATCH(FN, ...)                                                                      \
+  switch (p->g.w) {                                                                                 \
+    case 2: return FN<2>(__VA_ARGS__);   case 3: return FN<3>(__VA_ARGS__);                          \
+    case 4: return FN<4>(__VA_ARGS__);   case 5: return FN<5>(__VA_ARGS__);                          \
+    case 6: return FN<6>(__VA_ARGS__);   case 7: return FN<7>(__VA_ARGS__);                          \
+    case 8: return FN<8>(__VA_ARGS__);   case 9: return FN<9>(__VA_ARGS__);                          \
+    case 10: return FN<10>(__VA_ARGS__); case 11: return FN<11>(__VA_ARGS__);                        \
+    case 12: return FN<12>(__VA_ARGS__); case 13: return FN<13>(__VA_ARGS__);                        \
+    case 14: return FN<14>(__VA_ARGS__); case 15: return FN<15>(__VA_ARGS__);                        \
+    case 16: return FN<16>(__VA_ARGS__);                                                             \
+    default: return cudaErrorInvalidValue;                                                           \
+  }
+
+cudaError_t spread(const hb_nufft* p, const float2* c, long long c_ld, int nb, cudaStream_t st) {
+  HB_W_DISPATCH(spread_w, p, c, c_ld, nb, st)
+}
+cudaError_t interp(const hb_nufft* p, float2* c, long long c_ld, int nb, cudaStream_t st) {
+  HB_W_DISPATCH(interp_w, p, c, c_ld, nb, st)
+}
+
+long long nmodes(const hb_nufft* p) { return (long long)p->g.N[0] * p->g.N[1] * p->g.N[2]; }
+long long nfine(const hb_nufft* p) { return (long long)p->g.n[0] * p->g.n[1] * p->g.n[2]; }
+
+// nb <= maxbatch transforms: c [nb][K] (row pitch c_ld) -> f [nb][modes] (row pitch f_ld)
+int type1_batch(const hb_nufft* p, const float2* c, long long c_ld, float2* f, long long f_ld, int nb, int isign,
+                cudaStream_t st) {
+  HB_CUDA(cudaMemsetAsync(p->grid, 0, (size_t)nb * nfine(p) * sizeof(float2), st));
+  HB_CUDA(spread(p, c, c_ld, nb, st));
+  HB_CUDA(isign > 0 ? fft3<1>(p, p->grid, nb, st) : fft3<-1>(p, p->grid, nb, st));
+  dim3 grid((unsigned)((nmodes(p) + 255) / 256), nb);
+  {
+    LaunchScope ls(HB_KERNEL_NUFFT, st);
+    nufft_deconv_kernel<<<grid, 256, 0, st>>>(p->g, p->grid, p->corr, f, f_ld);
+  }
+  HB_CHECK_LAUNCH();
+  return HB_OK;
+}
+
+// nb <= maxbatch transforms: f [nb][modes] -> c [nb][K]
+int type2_batch(const hb_nufft* p, const float2* f, long long f_ld, float2* c, long long c_ld, int nb, int isign,
+                cudaStream_t st) {
+  HB_CUDA(cudaMemsetAsync(p->grid, 0, (size_t)nb * nfine(p) * sizeof(float2), st));
+  dim3 grid((unsigned)((nmodes(p) + 255) / 256), nb);
+  {
+    LaunchScope ls(HB_KERNEL_NUFFT, st);
+    nufft_precorrect_kernel<<<grid, 256, 0, st>>>(p->g, f, f_ld, p->corr, p->grid);
+  }
+  HB_CHECK_LAUNCH();
+  HB_CUDA(isign > 0 ? fft3<1>(p, p->grid, nb, st) : fft3<-1>(p, p->grid, nb, st));
+  HB_CUDA(interp(p, c, c_ld, nb, st));
+  return HB_OK;
+}
+
+void free_plan(hb_nufft* p) {
+  if (!p) return;
+  cudaFree(p->coords);
+  cudaFree(p->perm);
+  cudaFree(p->corr);
+  cudaFree(p->tw);
+  cudaFree(p->grid);
+  cudaFree(p->modes);
+  delete p;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_nufft_create(hb_nufft** out, int64_t nz, int64_t ny, int64_t nx, const float* coords, int64_t nsamples,
+                    double tol, int maxbatch, int device, void* stream) {
+  if (!out) return fail(HB_ERR_INVALID, "hb_nufft_create: null output");
+  *out = nullptr;
+  if (!coords || nsamples < 1 || nsamples > (int64_t)0x7fffffff)
+    return fail(HB_ERR_INVALID, "hb_nufft_create: need coords and 1 <= nsamples < 2^31");
+  if (!(tol > 0.0 && tol < 1.0)) return fail(HB_ERR_INVALID, "hb_nufft_create: tol must be in (0, 1)");
+  if (maxbatch < 1 || maxbatch > kNufftMaxBatch)
+    return fail(HB_ERR_INVALID, "hb_nufft_create: maxbatch must be in [1, " + std::to_string(kNufftMaxBatch) + "]");
+  const int64_t Nv[3] = {nz, ny, nx};
+  NufftGeom g{};
+  g.w = width_for_tol(tol);
+  g.beta = (float)(2.30 * g.w);
+  g.K = nsamples;
+  for (int a = 0; a < 3; ++a) {
+    int E = 0, S = 0;
+    const int64_t n = 2 * Nv[a];
+    if (Nv[a] < 1 || n > 320 || !team_length((int)n, &E, &S) || n < 2 * g.w)
+      return fail(HB_ERR_UNSUPPORTED, "hb_nufft_create: mode count " + std::to_string(Nv[a]) +
+                                          " unsupported (2N must be one of 8,16,32,64,128,256,96,160,192,320 and >= 2w)");
+    g.N[a] = (int)Nv[a];
+    g.n[a] = (int)n;
+    g.nb[a] = (g.n[a] + kNufftBin - 1) / kNufftBin;
+  }
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(HB_ERR_CUDA, "hb_nufft_create: cannot select device");
+  cudaStream_t st = (cudaStream_t)stream;
+  hb_nufft* p = new hb_nufft();
+  p->device = device;
+  p->g = g;
+  p->maxbatch = maxbatch;
+  const long long nbins = (long long)g.nb[0] * g.nb[1] * g.nb[2];
+  const long long vol = (long long)g.n[0] * g.n[1] * g.n[2];
+  const long long nm = (long long)g.N[0] * g.N[1] * g.N[2];
+  int* bin_of = nullptr;
+  int* counts = nullptr;
+  auto bail = [&](cudaError_t e, const char* what) {
+    cudaFree(bin_of);
+    cudaFree(counts);
+    free_plan(p);
+    return fail(HB_ERR_CUDA, std::string("hb_nufft_create: ") + what + ": " + cudaGetErrorString(e));
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&p->coords, 3 * nsamples * sizeof(float))) != cudaSuccess) return bail(e, "coords");
+  if ((e = cudaMalloc(&p->perm, nsamples * sizeof(int))) != cudaSuccess) return bail(e, "perm");
+  if ((e = cudaMalloc(&p->corr, (g.N[0] + g.N[1] + g.N[2]) * sizeof(float))) != cudaSuccess) return bail(e, "corr");
+  if ((e = cudaMalloc(&p->tw, (g.n[0] + g.n[1] + g.n[2]) * sizeof(float2))) != cudaSuccess) return bail(e, "tables");
+  if ((e = cudaMalloc(&p->grid, (size_t)maxbatch * vol * sizeof(float2))) != cudaSuccess) return bail(e, "fine grid");
+  if ((e = cudaMalloc(&p->modes, (size_t)maxbatch * nm * sizeof(float2))) != cudaSuccess) return bail(e, "modes");
+  if ((e = cudaMalloc(&bin_of, nsamples * sizeof(int))) != cudaSuccess) return bail(e, "bins");
+  if ((e = cudaMalloc(&counts, 2 * nbins * sizeof(int))) != cudaSuccess) return bail(e, "bins");
+
+  // host tables: 1/phi_hat per axis and the team twiddles of each fine-grid length
+  std::vector<float> corr;
+  for (int a = 0; a < 3; ++a)
+    for (int i = 0; i < g.N[a]; ++i) corr.push_back((float)(1.0 / phi_hat(i - g.N[a] / 2, g.n[a], g.w, 2.30 * g.w)));
+  std::vector<float2> tw;
+  for (int a = 0; a < 3; ++a) {
+    int E = 0, S = 0;
+    team_length(g.n[a], &E, &S);
+    for (int k1 = 0; k1 < E; ++k1)
+      for (int t = 0; t < S; ++t) {
+        const double ang = -2.0 * M_PI * (double)(t * k1) / (double)g.n[a];
+        tw.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
+      }
+  }
+  if ((e = cudaMemcpyAsync(p->corr, corr.data(), corr.size() * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return bail(e, "upload");
+  if ((e = cudaMemcpyAsync(p->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return bail(e, "upload");
+  if ((e = cudaMemcpyAsync(p->coords, coords, 3 * nsamples * sizeof(float), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+    return bail(e, "coords copy");
+  // counting sort of the samples by bin
+  if ((e = cudaMemsetAsync(counts, 0, nbins * sizeof(int), st)) != cudaSuccess) return bail(e, "memset");
+  const unsigned blocks = (unsigned)((nsamples + 255) / 256);
+  {
+    LaunchScope ls(HB_KERNEL_NUFFT, st);
+    nufft_bin_count_kernel<<<blocks, 256, 0, st>>>(g, p->coords, bin_of, counts);
+  }
+  {
+    LaunchScope ls(HB_KERNEL_NUFFT, st);
+    nufft_scan_kernel<<<1, 1024, 0, st>>>(counts, counts + nbins, (int)nbins);
+  }
+  {
+    LaunchScope ls(HB_KERNEL_NUFFT, st);
+    nufft_bin_scatter_kernel<<<blocks, 256, 0, st>>>(nsamples, bin_of, counts + nbins, p->perm);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return bail(e, "binning");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return bail(e, "binning");
+  cudaFree(bin_of);
+  cudaFree(counts);
+  *out = p;
+  return HB_OK;
+}
+
+int hb_nufft_destroy(hb_nufft* plan) {
+  if (!plan) return HB_OK;
+  DeviceGuard dg(plan->device);
+  free_plan(plan);
+  return HB_OK;
+}
+
+int hb_nufft_width(const hb_nufft* plan) { return plan ? plan->g.w : -1; }
+
+int hb_nufft_type1(const hb_nufft* plan, const void* c, void* f, int64_t ntransf, int isign, void* stream) {
+  if (!plan || !c || !f || ntransf < 0 || (isign != 1 && isign != -1))
+    return fail(HB_ERR_INVALID, "hb_nufft_type1: null argument, negative ntransf or isign not +-1");
+  DeviceGuard dg(plan->device);
+  const long long K = plan->g.K, nm = nmodes(plan);
+  for (int64_t t0 = 0; t0 < ntransf; t0 += plan->maxbatch) {
+    const int nb = (int)((ntransf - t0) < plan->maxbatch ? (ntransf - t0) : plan->maxbatch);
+    if (int r = type1_batch(plan, (const float2*)c + t0 * K, K, (float2*)f + t0 * nm, nm, nb, isign,
+                            (cudaStream_t)stream))
+      return r;
+  }
+  return HB_OK;
+}
+
+int hb_nufft_type2(const hb_nufft* plan, const void* f, void* c, int64_t ntransf, int isign, void* stream) {
+  if (!plan || !c || !f || ntransf < 0 || (isign != 1 && isign != -1))
+    return fail(HB_ERR_INVALID, "hb_nufft_type2: null argument, negative ntransf or isign not +-1");
+  DeviceGuard dg(plan->device);
+  const long long K = plan->g.K, nm = nmodes(plan);
+  for (int64_t t0 = 0; t0 < ntransf; t0 += plan->maxbatch) {
+    const int nb = (int)((ntransf - t0) < plan->maxbatch ? (ntransf - t0) : plan->maxbatch);
+    if (int r = type2_batch(plan, (const float2*)f + t0 * nm, nm, (float2*)c + t0 * K, K, nb, isign,
+                            (cudaStream_t)stream))
+      return r;
+  }
+  return HB_OK;
+}
+
+int hb_sense_adjoint_nufft(const hb_nufft* plan, const void* kdata, const void* smaps, const int64_t* coils,
+                           int64_t ncoil, void* out, int accumulate, void* stream) {
+  if (!plan || !kdata || !smaps || !out || ncoil < 0 || (ncoil > 0 && !coils))
+    return fail(HB_ERR_INVALID, "hb_sense_adjoint_nufft: null argument or negative ncoil");
+  for (int64_t b = 0; b < ncoil; ++b)
+    if (coils[b] < 0) return fail(HB_ERR_INVALID, "hb_sense_adjoint_nufft: negative coil index");
+  DeviceGuard dg(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long K = plan->g.K, nm = nmodes(plan);
+  const unsigned vb = (unsigned)((nm + 255) / 256);
+  if (ncoil == 0 && !accumulate) HB_CUDA(cudaMemsetAsync(out, 0, nm * sizeof(float2), st));
+  for (int64_t b0 = 0; b0 < ncoil; b0 += plan->maxbatch) {
+    const int nb = (int)((ncoil - b0) < plan->maxbatch ? (ncoil - b0) : plan->maxbatch);
+    if (int r = type1_batch(plan, (const float2*)kdata + b0 * K, K, plan->modes, nm, nb, +1, st)) return r;
+    CoilMaps maps{};
+    for (int b = 0; b < nb; ++b) maps.s[b] = (const float2*)smaps + coils[b0 + b] * nm;
+    {
+      LaunchScope ls(HB_KERNEL_NUFFT, st);
+      sense_coil_combine_kernel<<<vb, 256, 0, st>>>(plan->modes, nb, nm, maps, (float2*)out,
+                                                    (b0 > 0 || accumulate) ? 1 : 0);
+    }
+    HB_CHECK_LAUNCH();
+  }
+  return HB_OK;
+}
+
+int hb_sense_forward_nufft(const hb_nufft* plan, const void* x, const void* smaps, const int64_t* coils,
+                           int64_t ncoil, void* kdata, void* stream) {
+  if (!plan || !x || !smaps || !kdata || ncoil < 0 || (ncoil > 0 && !coils))
+    return fail(HB_ERR_INVALID, "hb_sense_forward_nufft: null argument or negative ncoil");
+  for (int64_t b = 0; b < ncoil; ++b)
+    if (coils[b] < 0) return fail(HB_ERR_INVALID, "hb_sense_forward_nufft: negative coil index");
+  DeviceGuard dg(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long K = plan->g.K, nm = nmodes(plan);
+  const unsigned vb = (unsigned)((nm + 255) / 256);
+  for (int64_t b0 = 0; b0 < ncoil; b0 += plan->maxbatch) {
+    const int nb = (int)((ncoil - b0) < plan->maxbatch ? (ncoil - b0) : plan->maxbatch);
+    CoilMaps maps{};
+    for (int b = 0; b < nb; ++b) maps.s[b] = (const float2*)smaps + coils[b0 + b] * nm;
+    {
+      LaunchScope ls(HB_KERNEL_NUFFT, st);
+      sense_coil_expand_kernel<<<vb, 256, 0, st>>>((const float2*)x, nb, nm, maps, plan->modes);
+    }
+    HB_CHECK_LAUNCH();
+    if (int r = type2_batch(plan, plan->modes, nm, (float2*)kdata + b0 * K, K, nb, -1, st)) return r;
+  }
+  return HB_OK;
+}
+
+}  // extern "C"

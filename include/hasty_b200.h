@@ -198,6 +198,44 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
                               int64_t out_ldz, int64_t out_ldy, const void* mul, int accumulate,
                               const float* packed_diag, void* stream);
 
+/* ---- Non-uniform FFT (types 1 and 2) and the SENSE operators around it ----
+ *
+ * Replaces hasty::fft::CUDANufft (cufinufft plan + setpts + execute,
+ * lib/fft/nufft.cpp:540-767, declared nufft.ixx:108-160) and the coil loops of the SENSE
+ * forward/adjoint operators that use it (lib/mri/sense.ixx:426-497).  Same conventions:
+ * coords is float32 [3][nsamples] on the device, row a pairing with image axis a
+ * (nufft.cpp:192-197), in radians (2*pi periodic); modes are centred,
+ * k_a = i_a - floor(N_a / 2) for array index i_a, arrays [nz][ny][nx];
+ *   type 1:  f[k] = sum_j c[j] exp(isign * i * k . x_j)      (reference: isign = +1)
+ *   type 2:  c[j] = sum_k f[k] exp(isign * i * k . x_j)      (reference: isign = -1)
+ * Method: exponential-of-semicircle gridding kernel with upsampling 2 (the published
+ * method of finufft); kernel width w = ceil(log10(1/tol)) + 1 fine-grid cells.
+ * 2*N_a must be one of 8, 16, 32, 64, 128, 256, 96, 160, 192, 320 and >= 2w.
+ * Type 1 accumulates with atomics, so its last bits vary from run to run.
+ *
+ * hb_nufft_create copies coords, sorts the samples by fine-grid bin and allocates the
+ * fine grids of `maxbatch` (1..32) transforms plus as many mode arrays; it synchronises
+ * `stream`.  Transforms run in batches of maxbatch.  c is [ntransf][nsamples], f is
+ * [ntransf][nz][ny][nx]. */
+typedef struct hb_nufft hb_nufft;
+int hb_nufft_create(hb_nufft** plan, int64_t nz, int64_t ny, int64_t nx, const float* coords, int64_t nsamples,
+                    double tol, int maxbatch, int device, void* stream);
+int hb_nufft_destroy(hb_nufft* plan);
+/* Kernel width w (fine-grid cells) the plan uses. */
+int hb_nufft_width(const hb_nufft* plan);
+int hb_nufft_type1(const hb_nufft* plan, const void* c, void* f, int64_t ntransf, int isign, void* stream);
+int hb_nufft_type2(const hb_nufft* plan, const void* f, void* c, int64_t ntransf, int isign, void* stream);
+
+/* SENSE adjoint: out (+)= sum_b conj(S[coils[b]]) * type1(kdata[b]) (isign +1), kdata
+ * [ncoil][nsamples], smaps [*][nz][ny][nx], coils a HOST array of ncoil map indices;
+ * accumulate = 0 overwrites out.  The CG right-hand side of the reference's SENSE
+ * reconstructions. */
+int hb_sense_adjoint_nufft(const hb_nufft* plan, const void* kdata, const void* smaps, const int64_t* coils,
+                           int64_t ncoil, void* out, int accumulate, void* stream);
+/* SENSE forward: kdata[b] = type2(S[coils[b]] * x) (isign -1). */
+int hb_sense_forward_nufft(const hb_nufft* plan, const void* x, const void* smaps, const int64_t* coils,
+                           int64_t ncoil, void* kdata, void* stream);
+
 /* ---- measurement hooks (no counterpart in the reference; used by benchmarks) ----
  * Kernel kinds for the profile counters. */
 #define HB_KERNEL_EXPAND_FWD_X 0   /* pass A */
@@ -205,7 +243,8 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
 #define HB_KERNEL_INV_X_COMBINE 2  /* pass C */
 #define HB_KERNEL_CG_UPDATE 3      /* CG vector updates / reductions */
 #define HB_KERNEL_DIAG 4           /* diagonal construction / packing */
-#define HB_KERNEL_KINDS 5
+#define HB_KERNEL_NUFFT 5          /* NUFFT: binning, spreading, fine-grid FFT, interpolation, SENSE */
+#define HB_KERNEL_KINDS 6
 
 /* Total number of kernels this library has launched in this process. */
 uint64_t hb_launch_count(void);

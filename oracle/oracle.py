@@ -22,6 +22,8 @@ LibTorch).  File references below are paths inside the reference project:
 * ``lib/op/opalgs.cpp:50-96``  ``ConjugateGradient::run`` (r = b - A x, p = z, the
   tol test on sqrt(rz), the positive-definiteness check) applied to ``A + lambda*I``
   (``python/python/hastypy/base/torch_opalg.py:49-61``).
+* ``lib/fft/nufft.cpp:540-767`` the type-1 / type-2 NUFFTs of ``CUDANufft`` and the SENSE
+  forward / adjoint around them (``lib/mri/sense.ixx:426-497``), as direct NUDFTs.
 * ``lib/fft/nufft.cpp:410-767`` / ``:785-920`` explicit NUFFT normal op on the N grid
   (type-2 then type-1, each /sqrt(prod(N))), evaluated as a dense direct NUDFT.
   ``Toeplitz = explicit / 2^3`` in 3D because of the two different grid scalings.
@@ -118,6 +120,46 @@ def explicit_normal(x, coords, weights=None):
     # type 1: y_k = sum_j f_j exp(+i k.c_j)
     y = np.einsum("j,jz,jy,jx->zyx", f, ez, ey, ex, optimize=True)
     return y / float(np.prod(N))
+
+
+def nudft_type1(coords, c, nmodes, isign=+1):
+    """Direct FP64 type-1 NUDFT, the transform ``hasty::fft::CUDANufft`` type 1 computes
+    through cufinufft (``lib/fft/nufft.cpp:640-700``; options ``nufft.ixx:46-48``):
+    f[t, k] = sum_j c[t, j] exp(isign * i * k . x_j), centred modes k = i - n//2,
+    c [ntransf, K] -> f [ntransf, *nmodes]."""
+    coords = np.asarray(coords, np.float64)
+    c = np.atleast_2d(np.asarray(c, np.complex128))
+    k = [np.arange(n) - n // 2 for n in nmodes]
+    e = [np.exp(isign * 1j * np.outer(coords[a], k[a])) for a in range(3)]
+    return np.einsum("tj,jz,jy,jx->tzyx", c, e[0], e[1], e[2], optimize=True)
+
+
+def nudft_type2(coords, f, isign=-1):
+    """Direct FP64 type-2 NUDFT (``lib/fft/nufft.cpp:702-767``):
+    c[t, j] = sum_k f[t, k] exp(isign * i * k . x_j), f [ntransf, *nmodes] -> c [ntransf, K]."""
+    coords = np.asarray(coords, np.float64)
+    f = np.asarray(f, np.complex128)
+    if f.ndim == 3:
+        f = f[None]
+    k = [np.arange(n) - n // 2 for n in f.shape[1:]]
+    e = [np.exp(isign * 1j * np.outer(coords[a], k[a])) for a in range(3)]
+    return np.einsum("tzyx,jz,jy,jx->tj", f, e[0], e[1], e[2], optimize=True)
+
+
+def sense_adjoint(coords, kdata, smaps, coils=None):
+    """SENSE adjoint with the type-1 NUFFT (``lib/mri/sense.ixx:426-497``):
+    out = sum_b conj(S[coils[b]]) * type1(kdata[b])."""
+    smaps = np.asarray(smaps, np.complex128)
+    coils = range(smaps.shape[0]) if coils is None else coils
+    imgs = nudft_type1(coords, kdata, smaps.shape[1:], +1)
+    return sum(np.conj(smaps[c]) * imgs[b] for b, c in enumerate(coils))
+
+
+def sense_forward(coords, x, smaps, coils=None):
+    """SENSE forward with the type-2 NUFFT: kdata[b] = type2(S[coils[b]] * x)."""
+    smaps = np.asarray(smaps, np.complex128)
+    coils = range(smaps.shape[0]) if coils is None else coils
+    return nudft_type2(coords, np.stack([smaps[c] * x for c in coils]), -1)
 
 
 def vdot(a, b):

@@ -120,3 +120,32 @@ def test_cg_tol_and_iter_zero():
     assert n == 0 and np.all(x == 0)
     x, n = O.conjugate_gradient(lambda v: 2 * v, b, iters=10, tol=1e-9)
     assert n == 1 and np.allclose(x, 0.5)
+
+
+def test_nudft_pair_pinned_to_the_explicit_normal(golden):
+    """The direct type-1 / type-2 NUDFTs compose to the explicit normal operator that the
+    reference's dense builder pins (type 2 with isign -1, type 1 with isign +1, over
+    prod(N)), and type 2 (-1) is the adjoint of type 1 (+1)."""
+    x = golden["x_cnm"]
+    c = golden["coords"][:, :30].astype(np.float64)
+    y = O.nudft_type1(c, O.nudft_type2(c, x, -1), x.shape, +1)[0] / np.prod(x.shape)
+    assert O.rel_l2(y, O.explicit_normal(x, c)) < 1e-12
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape)
+    k = rng.standard_normal((1, 30)) + 1j * rng.standard_normal((1, 30))
+    lhs = np.vdot(O.nudft_type2(c, f, -1).ravel(), k.ravel())
+    rhs = np.vdot(f.ravel(), O.nudft_type1(c, k, x.shape, +1).ravel())
+    assert abs(lhs - rhs) < 1e-10 * abs(rhs)
+
+
+def test_sense_adjoint_forward_oracle_pair():
+    rng = np.random.default_rng(6)
+    shape, K = (4, 3, 5), 40
+    c = rng.uniform(-np.pi, np.pi, (3, K))
+    sm = rng.standard_normal((3,) + shape) + 1j * rng.standard_normal((3,) + shape)
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    kd = rng.standard_normal((2, K)) + 1j * rng.standard_normal((2, K))
+    coils = [2, 0]
+    lhs = np.vdot(O.sense_forward(c, x, sm, coils).ravel(), kd.ravel())
+    rhs = np.vdot(x.ravel(), O.sense_adjoint(c, kd, sm, coils).ravel())
+    assert abs(lhs - rhs) < 1e-10 * abs(rhs)
