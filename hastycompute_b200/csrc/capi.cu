@@ -26,6 +26,15 @@ struct hb_plan {
   int plane_variant = -1;  // plane-pass schedule chosen by hb_plan_autotune (-1: default)
 };
 
+namespace hb {
+void plan_geometry(const ::hb_plan* p, int* N, int* device) {
+  N[0] = p->N0;
+  N[1] = p->N1;
+  N[2] = p->N2;
+  *device = p->device;
+}
+}  // namespace hb
+
 namespace {
 
 // Supported axis lengths and their row in the launcher tables.

@@ -222,6 +222,7 @@ template <int DIR> struct Dft<12, DIR> : DftMixed<3, 4, DIR> {};
 template <int DIR> struct Dft<20, DIR> : DftMixed<5, 4, DIR> {};
 template <int DIR> struct Dft<24, DIR> : DftMixed<3, 8, DIR> {};
 template <int DIR> struct Dft<40, DIR> : DftMixed<5, 8, DIR> {};
+template <int DIR> struct Dft<32, DIR> : DftMixed<4, 8, DIR> {};
 
 // DFT of size R whose inputs v[R/2..R-1] are zero (they are not read).
 // X[2k] = DFT_{R/2}(v)[k];  X[2k+1] = DFT_{R/2}(v[n] * w_R^n)[k]
@@ -272,6 +273,7 @@ template <> struct TeamCfg<96> { static constexpr int E = 24, S = 4; };
 template <> struct TeamCfg<160> { static constexpr int E = 40, S = 4; };
 template <> struct TeamCfg<192> { static constexpr int E = 24, S = 8; };
 template <> struct TeamCfg<320> { static constexpr int E = 40, S = 8; };
+template <> struct TeamCfg<512> { static constexpr int E = 32, S = 16; };
 
 // Shared-memory float2 slots one team needs for its exchange buffer.  The stride is
 // chosen so that teams sharing a half-warp land on disjoint banks.

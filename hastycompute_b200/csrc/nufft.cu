@@ -1,7 +1,8 @@
 // C ABI of the NUFFT (types 1 and 2) and the SENSE forward/adjoint around it
 // (include/hasty_b200.h, section "Non-uniform FFT").  Replaces the cufinufft plans of
-// hasty::fft::CUDANufft (lib/fft/nufft.cpp:540-767, declared nufft.ixx:108-160) and the
-// coil loops of the SENSE operators that use them (lib/mri/sense.ixx:426-497).
+// hasty::fft::CUDANufft (lib/fft/nufft.cpp:540-767, declared nufft.ixx:108-160), the
+// coil loops of the SENSE operators that use them (lib/mri/sense.ixx:426-497) and the
+// NUFFT construction of the Toeplitz diagonal (build_diagonal_base, nufft.cpp:932-971).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -41,6 +42,7 @@ bool team_length(int L, int* E, int* S) {
     case 160: *E = 40; *S = 4; return true;
     case 192: *E = 24; *S = 8; return true;
     case 320: *E = 40; *S = 8; return true;
+    case 512: *E = 32; *S = 16; return true;
     default: return false;
   }
 }
@@ -117,6 +119,7 @@ cudaError_t contig_any(int L, float2* d, long long nlines, const float2* tw, cud
     case 160: return lines_contig<160, DIR>(d, nlines, tw, st);
     case 192: return lines_contig<192, DIR>(d, nlines, tw, st);
     case 320: return lines_contig<320, DIR>(d, nlines, tw, st);
+    case 512: return lines_contig<512, DIR>(d, nlines, tw, st);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -135,19 +138,40 @@ cudaError_t strided_any(int L, float2* d, long long rs, int ncols, int ny, long 
     case 160: return lines_strided<160, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
     case 192: return lines_strided<192, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
     case 320: return lines_strided<320, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
+    case 512: return lines_strided<512, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
+// nt grids [n0][n1][n2] in place; tw: team tables of n0, n1, n2 back to back
+template <int DIR>
+cudaError_t fft3_grid(int n0, int n1, int n2, const float2* tw, float2* grid, int nt, cudaStream_t st) {
+  const long long vol = (long long)n0 * n1 * n2;
+  cudaError_t e = contig_any<DIR>(n2, grid, (long long)nt * n0 * n1, tw + n0 + n1, st);
+  if (e != cudaSuccess) return e;
+  e = strided_any<DIR>(n1, grid, n2, n2, n0, (long long)n1 * n2, nt, vol, tw + n0, st);
+  if (e != cudaSuccess) return e;
+  return strided_any<DIR>(n0, grid, (long long)n1 * n2, n2, n1, n2, nt, vol, tw, st);
+}
+
 template <int DIR>
 cudaError_t fft3(const hb_nufft* p, float2* grid, int nt, cudaStream_t st) {
-  const int n0 = p->g.n[0], n1 = p->g.n[1], n2 = p->g.n[2];
-  const long long vol = (long long)n0 * n1 * n2;
-  cudaError_t e = contig_any<DIR>(n2, grid, (long long)nt * n0 * n1, p->tw + n0 + n1, st);
-  if (e != cudaSuccess) return e;
-  e = strided_any<DIR>(n1, grid, n2, n2, n0, (long long)n1 * n2, nt, vol, p->tw + n0, st);
-  if (e != cudaSuccess) return e;
-  return strided_any<DIR>(n0, grid, (long long)n1 * n2, n2, n1, n2, nt, vol, p->tw, st);
+  return fft3_grid<DIR>(p->g.n[0], p->g.n[1], p->g.n[2], p->tw, grid, nt, st);
+}
+
+// Team twiddle tables of the three lengths, back to back (forward sign, FP64 rounded).
+std::vector<float2> team_tables(const int* n) {
+  std::vector<float2> tw;
+  for (int a = 0; a < 3; ++a) {
+    int E = 0, S = 0;
+    team_length(n[a], &E, &S);
+    for (int k1 = 0; k1 < E; ++k1)
+      for (int t = 0; t < S; ++t) {
+        const double ang = -2.0 * M_PI * (double)(t * k1) / (double)n[a];
+        tw.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
+      }
+  }
+  return tw;
 }
 
 template <int W>
@@ -250,9 +274,10 @@ int hb_nufft_create(hb_nufft** out, int64_t nz, int64_t ny, int64_t nx, const fl
   for (int a = 0; a < 3; ++a) {
     int E = 0, S = 0;
     const int64_t n = 2 * Nv[a];
-    if (Nv[a] < 1 || n > 320 || !team_length((int)n, &E, &S) || n < 2 * g.w)
+    if (Nv[a] < 1 || n > 512 || !team_length((int)n, &E, &S) || n < 2 * g.w)
       return fail(HB_ERR_UNSUPPORTED, "hb_nufft_create: mode count " + std::to_string(Nv[a]) +
-                                          " unsupported (2N must be one of 8,16,32,64,128,256,96,160,192,320 and >= 2w)");
+                                          " unsupported (2N must be one of 8,16,32,64,128,256,512,96,160,192,320 "
+                                          "and >= 2w)");
     g.N[a] = (int)Nv[a];
     g.n[a] = (int)n;
     g.nb[a] = (g.n[a] + kNufftBin - 1) / kNufftBin;
@@ -289,16 +314,7 @@ int hb_nufft_create(hb_nufft** out, int64_t nz, int64_t ny, int64_t nx, const fl
   std::vector<float> corr;
   for (int a = 0; a < 3; ++a)
     for (int i = 0; i < g.N[a]; ++i) corr.push_back((float)(1.0 / phi_hat(i - g.N[a] / 2, g.n[a], g.w, 2.30 * g.w)));
-  std::vector<float2> tw;
-  for (int a = 0; a < 3; ++a) {
-    int E = 0, S = 0;
-    team_length(g.n[a], &E, &S);
-    for (int k1 = 0; k1 < E; ++k1)
-      for (int t = 0; t < S; ++t) {
-        const double ang = -2.0 * M_PI * (double)(t * k1) / (double)g.n[a];
-        tw.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
-      }
-  }
+  const std::vector<float2> tw = team_tables(g.n);
   if ((e = cudaMemcpyAsync(p->corr, corr.data(), corr.size() * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return bail(e, "upload");
   if ((e = cudaMemcpyAsync(p->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, st)) != cudaSuccess)
@@ -413,6 +429,65 @@ int hb_sense_forward_nufft(const hb_nufft* plan, const void* x, const void* smap
     if (int r = type2_batch(plan, plan->modes, nm, (float2*)kdata + b0 * K, K, nb, -1, st)) return r;
   }
   return HB_OK;
+}
+
+int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsamples, double tol, float* packed,
+                        void* T_complex, void* stream) {
+  if (!plan || !coords || nsamples < 1) return fail(HB_ERR_INVALID, "hb_diag_build_nufft: null plan or no samples");
+  if (!packed && !T_complex) return fail(HB_ERR_INVALID, "hb_diag_build_nufft: no output requested");
+  int N[3], dev = 0;
+  plan_geometry(plan, N, &dev);
+  DeviceGuard dg(dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int M[3] = {2 * N[0], 2 * N[1], 2 * N[2]};
+  const long long vol = (long long)M[0] * M[1] * M[2];
+  hb_nufft* np = nullptr;
+  // type 1 over the 2x grid's modes: psf(d) = sum_j exp(+i c_j . d), d in [-N, N)
+  if (int r = hb_nufft_create(&np, M[0], M[1], M[2], coords, nsamples, tol, 1, dev, stream)) return r;
+  float2* ones = nullptr;
+  float2* tw = nullptr;
+  int rc = HB_OK;
+  auto cuda_fail = [&](cudaError_t e, const char* what) {
+    rc = fail(HB_ERR_CUDA, std::string("hb_diag_build_nufft: ") + what + ": " + cudaGetErrorString(e));
+    return rc;
+  };
+  do {
+    cudaError_t e;
+    if ((e = cudaMalloc(&ones, nsamples * sizeof(float2))) != cudaSuccess) { cuda_fail(e, "alloc"); break; }
+    const std::vector<float2> tables = team_tables(M);
+    if ((e = cudaMalloc(&tw, tables.size() * sizeof(float2))) != cudaSuccess) { cuda_fail(e, "alloc"); break; }
+    if ((e = cudaMemcpyAsync(tw, tables.data(), tables.size() * sizeof(float2), cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess) {
+      cuda_fail(e, "upload");
+      break;
+    }
+    {
+      LaunchScope ls(HB_KERNEL_DIAG, st);
+      fill_c64_kernel<<<(unsigned)((nsamples + 255) / 256), 256, 0, st>>>(ones, nsamples, make_float2(1.f, 0.f));
+    }
+    if ((rc = type1_batch(np, ones, nsamples, np->modes, vol, 1, +1, st)) != HB_OK) break;
+    // the fine grid is free again: T in circulant layout there, then the forward FFT
+    float2* T = np->grid;
+    {
+      LaunchScope ls(HB_KERNEL_DIAG, st);
+      ifftshift3_scale_kernel<<<(unsigned)((vol + 255) / 256), 256, 0, st>>>(np->modes, M[0], M[1], M[2],
+                                                                             (float)(1.0 / (double)vol), T);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) { cuda_fail(e, "kernel launch"); break; }
+    if ((e = fft3_grid<-1>(M[0], M[1], M[2], tw, T, 1, st)) != cudaSuccess) { cuda_fail(e, "fft"); break; }
+    if (packed && (rc = hb_diag_pack(plan, T, packed, stream)) != HB_OK) break;
+    if (T_complex &&
+        (e = cudaMemcpyAsync(T_complex, T, vol * sizeof(float2), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) {
+      cuda_fail(e, "copy");
+      break;
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) cuda_fail(e, "sync");
+  } while (false);
+  if (rc != HB_OK) cudaStreamSynchronize(st);
+  cudaFree(ones);
+  cudaFree(tw);
+  hb_nufft_destroy(np);
+  return rc;
 }
 
 }  // extern "C"

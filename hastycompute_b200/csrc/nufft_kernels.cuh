@@ -206,6 +206,23 @@ __global__ void nufft_precorrect_kernel(NufftGeom g, const float2* f, long long 
   grid[(long long)blockIdx.y * g.n[0] * g.n[1] * g.n[2] + cell] = cscale(f[(long long)blockIdx.y * f_ld + m], s);
 }
 
+// ---- Toeplitz diagonal through the NUFFT ----
+__global__ void fill_c64_kernel(float2* a, long long n, float2 v) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+// Circulant (ifftshift) layout of a centred [M0][M1][M2] array, scaled:
+// out[n] = s * in[(n + M/2) mod M] per axis (offset d = n for n < M/2, n - M otherwise).
+__global__ void ifftshift3_scale_kernel(const float2* in, int M0, int M1, int M2, float s, float2* out) {
+  const long long nv = (long long)M0 * M1 * M2;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const int n2 = (int)(i % M2), n1 = (int)((i / M2) % M1), n0 = (int)(i / ((long long)M1 * M2));
+  const int c0 = (n0 + M0 / 2) % M0, c1 = (n1 + M1 / 2) % M1, c2 = (n2 + M2 / 2) % M2;
+  out[i] = cscale(in[((long long)c0 * M1 + c1) * M2 + c2], s);
+}
+
 // ---- SENSE around the NUFFT ----
 constexpr int kNufftMaxBatch = 32;  // transforms per batch (coil-map pointers by value)
 struct CoilMaps {

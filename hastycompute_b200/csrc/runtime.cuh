@@ -16,6 +16,9 @@
 
 namespace hb {
 
+// Image size and device of a Toeplitz plan (defined with struct hb_plan).
+void plan_geometry(const ::hb_plan* plan, int* N, int* device);
+
 // Message of the last failure on this thread (hb_last_error).
 inline thread_local std::string g_err;
 

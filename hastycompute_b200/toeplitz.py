@@ -109,9 +109,12 @@ class ToeplitzPlan:
         return chosen.value, ms.value
 
     # ---------------------------------------------------------------- diagonal ----
-    def build_diagonal(self, coords, want_complex=False):
-        """FP64 construction of T from a trajectory coords [3, K] float32 (radians).
+    def build_diagonal(self, coords, want_complex=False, method="exact", tol=1e-6):
+        """Construction of T from a trajectory coords [3, K] float32 (radians).
 
+        method "exact": FP64 direct sum (``hb_diag_build``); "nufft": the reference's own
+        construction through a type-1 NUFFT at tolerance ``tol`` (``hb_diag_build_nufft``,
+        ``nufft.cpp:932-971``), much faster for long trajectories.
         Returns the packed diagonal (float32) and, if requested, the reference-layout
         complex64 T [2nz, 2ny, 2nx]."""
         if coords.dtype != torch.float32 or coords.dim() != 2 or coords.shape[0] != 3:
@@ -120,10 +123,16 @@ class ToeplitzPlan:
         K = coords.shape[1]
         packed = torch.empty(self.packed_numel(), dtype=torch.float32, device=self.device)
         T = torch.empty(self.grid, dtype=torch.complex64, device=self.device) if want_complex else None
-        nb = self.lib.hb_diag_build_workspace_bytes(self._h, K)
-        ws = torch.empty(int(nb), dtype=torch.uint8, device=self.device)
-        capi.check(self.lib.hb_diag_build(self._h, _ptr(coords), K, _ptr(packed), _ptr(T), _ptr(ws), nb,
-                                          _stream_ptr(self.device)))
+        if method == "nufft":
+            capi.check(self.lib.hb_diag_build_nufft(self._h, _ptr(coords), K, float(tol), _ptr(packed), _ptr(T),
+                                                    _stream_ptr(self.device)))
+        elif method == "exact":
+            nb = self.lib.hb_diag_build_workspace_bytes(self._h, K)
+            ws = torch.empty(int(nb), dtype=torch.uint8, device=self.device)
+            capi.check(self.lib.hb_diag_build(self._h, _ptr(coords), K, _ptr(packed), _ptr(T), _ptr(ws), nb,
+                                              _stream_ptr(self.device)))
+        else:
+            raise RuntimeError(f"unknown diagonal method {method!r} (exact or nufft)")
         return (packed, T) if want_complex else packed
 
     def pack_diagonal(self, T):

@@ -232,6 +232,16 @@ int hb_nufft_type2(const hb_nufft* plan, const void* f, void* c, int64_t ntransf
  * reconstructions. */
 int hb_sense_adjoint_nufft(const hb_nufft* plan, const void* kdata, const void* smaps, const int64_t* coils,
                            int64_t ncoil, void* out, int accumulate, void* stream);
+/* Toeplitz diagonal through the NUFFT, the reference's own construction
+ * (build_diagonal_base, lib/fft/nufft.cpp:932-971, at tolerance `tol`): the PSF is a
+ * type-1 NUFFT of unit weights onto the 2x grid's modes, shifted to circulant layout and
+ * scaled by 1/prod(2N), then FFT'd.  Same outputs as hb_diag_build (packed and/or the
+ * complex T [2nz][2ny][2nx]) to the NUFFT tolerance instead of FP64-exact, in
+ * milliseconds instead of seconds.  Allocates its NUFFT plan (a (4nz)(4ny)(4nx)
+ * complex64 fine grid) for the duration of the call and synchronises `stream`. */
+int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsamples, double tol, float* packed,
+                        void* T_complex, void* stream);
+
 /* SENSE forward: kdata[b] = type2(S[coils[b]] * x) (isign -1). */
 int hb_sense_forward_nufft(const hb_nufft* plan, const void* x, const void* smaps, const int64_t* coils,
                            int64_t ncoil, void* kdata, void* stream);

@@ -152,3 +152,20 @@ def test_cudanufft_mirror_and_errors(cuda):
     with pytest.raises(capi.HastyError) as e:
         plan.type1(_c64(c, cuda), isign=0)
     assert e.value.code == capi.HB_ERR_INVALID
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (8, 16, 32), (32, 32, 32)])
+def test_diagonal_through_the_nufft_matches_the_exact_build(cuda, shape):
+    """hb_diag_build_nufft (the reference's NUFFT construction, tol 1e-6) against the
+    FP64-exact hb_diag_build: complex T and the packed diagonal within 1e-5."""
+    coords = torch.from_numpy(_coords(4000, 19)).to(cuda)
+    plan = ToeplitzPlan(shape, cuda)
+    pe, Te = plan.build_diagonal(coords, want_complex=True)
+    pn, Tn = plan.build_diagonal(coords, want_complex=True, method="nufft", tol=1e-6)
+    assert O.rel_l2(_np(Tn), _np(Te)) < 1e-5
+    assert float((pn - pe).norm() / pe.norm()) < 1e-5
+    # against the oracle too
+    T = O.toeplitz_diagonal(coords.cpu().numpy().astype(np.float64), shape)
+    assert O.rel_l2(_np(Tn), T) < 1e-5
+    with pytest.raises(RuntimeError, match="method"):
+        plan.build_diagonal(coords, method="fast")
