@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--rates", default="1,2,4", help="serve: arrival rates (jobs/s)")
     ap.add_argument("--duration", type=float, default=30.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--diag", default="nufft", choices=["nufft", "exact"],
+                    help="Toeplitz diagonal construction: the reference's NUFFT route (tol 1e-6) or FP64-exact")
     return ap.parse_args()
 
 
@@ -206,7 +208,7 @@ def make_job_mix(a, dev, njobs, plans):
             plans[shape] = ToeplitzPlan(shape, dev)
         plan = plans[shape]
         coords = torch.from_numpy(synth.kooshball(spokes, a.samples, frame=j % 7, nframes=7))
-        packed = plan.build_diagonal(coords).unsqueeze(0)
+        packed = plan.build_diagonal(coords, method=a.diag).unsqueeze(0)
         sm = synth.coil_maps_torch(ncoil, shape, seed=1000 + j, device=dev)
         b = torch.randn((nframes,) + shape, dtype=torch.complex64, device=dev, generator=g)
         jobs.append({"shape": shape, "smaps": sm, "packed": packed, "b": b, "frames": nframes, "coils": ncoil,
@@ -375,7 +377,7 @@ def main():
     packed = torch.empty((a.frames, plan.packed_numel()), dtype=torch.float32, device=dev)
     for f in range(a.frames):
         coords = torch.from_numpy(synth.kooshball(a.spokes, a.samples, frame=f, nframes=a.frames))
-        packed[f] = plan.build_diagonal(coords)
+        packed[f] = plan.build_diagonal(coords, method=a.diag)
     torch.cuda.synchronize()
     t_diag = time.perf_counter() - t_setup
     diag_index = [s // a.encodings for s in range(nsys)]
@@ -474,8 +476,15 @@ def main():
     dom = max(("expand_fwd_x", "plane_yz", "inv_x_combine"), key=lambda k: prof[k][0])
     dms = prof[dom][0] / max(1, prof[dom][1])
     achieved = alg[dom] / (dms / 1000.0) / 1e9
+    # DRAM bytes (read + write) per (system, coil) slot of each pass, measured by ncu on one
+    # 16-coil system at 128^3 (profiles/passes_128c16_ncu_v3.md); a launch's traffic grows
+    # in proportion to its slots, so a full launch is that figure x slots
+    traffic_per_slot = {"expand_fwd_x": 766.4e6 / 16, "plane_yz": 1084.0e6 / 16, "inv_x_combine": 839.6e6 / 16}
+    traffic = traffic_per_slot[dom] * C * nsys if a.n == 128 else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_source": peak_src, "traffic": None,
+                "frac": achieved / hbm, "peak_source": peak_src, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read+write of one 16-slot launch, scaled by slots"
+                if traffic is not None else None,
                 "alg_bytes_per_launch": alg[dom], "ms_per_launch": dms}
     # whole-apply yardstick: (18C + 10) * U bytes per normal-op apply
     b_alg = (18 * C + 10) * U
@@ -495,7 +504,7 @@ def main():
             "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic (seeded)", "config": workload_config(a),
             "cg_solves_per_s": value / (a.iters + 1), "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "apply_yardstick": yard, "kernels": per_kernel, "cpu_baseline": cpu,
-            "clocks": clk, "setup_s": {"diagonals": t_diag},
+            "clocks": clk, "setup_s": {"diagonals": t_diag, "diagonal_method": a.diag},
         }
         print(json.dumps(line), flush=True)
     if pg:
