@@ -40,7 +40,7 @@ class HbSystem(ctypes.Structure):
     """struct hb_system (include/hasty_b200.h)."""
     _fields_ = [("x", ctypes.c_void_p), ("out", ctypes.c_void_p), ("b", ctypes.c_void_p),
                 ("smaps", ctypes.c_void_p), ("coils", ctypes.POINTER(ctypes.c_int64)), ("ncoil", ctypes.c_int64),
-                ("packed_diag", ctypes.c_void_p), ("lam", ctypes.c_float)]
+                ("packed_diag", ctypes.c_void_p), ("lam", ctypes.c_float), ("precond", ctypes.c_void_p)]
 
 
 P_sys = ctypes.POINTER(HbSystem)
@@ -82,6 +82,9 @@ SIGNATURES = {
     "hb_sense_adjoint_nufft": (c_int, [c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, c_int, c_void_p]),
     "hb_diag_build_nufft": (c_int, [c_void_p, c_void_p, c_i64, c_double, c_void_p, c_void_p, c_void_p]),
     "hb_sense_forward_nufft": (c_int, [c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, c_void_p]),
+    "hb_precond_build": (c_int, [c_void_p, c_void_p, c_i64, c_double, c_void_p, P_i64, c_i64, c_float, c_void_p,
+                                 c_void_p]),
+    "hb_precond_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "hb_launch_count": (ctypes.c_uint64, []),
     "hb_profile_start": (c_int, []),
     "hb_profile_stop": (c_int, [ctypes.POINTER(c_double), P_i64, c_int]),

@@ -13,6 +13,7 @@
 #include "../../include/hasty_b200.h"
 #include "cg_kernels.cuh"
 #include "diag_kernels.cuh"
+#include "fft3_launch.cuh"
 #include "runtime.cuh"
 #include "toeplitz_kernels.cuh"
 
@@ -33,6 +34,7 @@ void plan_geometry(const ::hb_plan* p, int* N, int* device) {
   N[2] = p->N2;
   *device = p->device;
 }
+const float2* plan_image_tables(const ::hb_plan* p) { return p->tables + p->to.total; }
 }  // namespace hb
 
 namespace {
@@ -265,6 +267,7 @@ int check_plan(const hb_plan* p) {
 // the host.
 struct TableLayout {
   size_t sys_x_init, sys_x_iter, sys_out, sys_smaps, sys_diag, cg_x, cg_b;  // pointer arrays
+  size_t sys_pdiag;                                                           // pointer array
   size_t sys_lambda;                                                          // float array
   size_t slot_sys, slot_coil, sys_slot0, sys_nslot;                           // int arrays
   size_t bytes;
@@ -285,6 +288,7 @@ TableLayout table_layout(int64_t g, int64_t slots) {
   L.sys_diag = take(8 * g);
   L.cg_x = take(8 * g);
   L.cg_b = take(8 * g);
+  L.sys_pdiag = take(8 * g);
   L.sys_lambda = take(4 * g);
   L.slot_sys = take(4 * slots);
   L.slot_coil = take(4 * slots);
@@ -299,7 +303,7 @@ struct GroupWs {
   char* tables;
   TableLayout L;
   // CG state (null when not a CG group)
-  float2 *r, *pv, *ap;
+  float2 *r, *pv, *ap, *z;
   double *rz, *pap, *rr;
   int *status, *active, *iters_done, *iter;
 };
@@ -314,6 +318,7 @@ GroupWs carve_group(Arena& ar, const hb_plan* p, int64_t g, int64_t slots, int i
     w.r = ar.take<float2>(g * nv);
     w.pv = ar.take<float2>(g * nv);
     w.ap = ar.take<float2>(g * nv);
+    w.z = ar.take<float2>(g * nv);
     w.rz = ar.take<double>(g * (size_t)(iters + 1));
     w.pap = ar.take<double>(g * (size_t)npap_blocks(p));
     w.rr = ar.take<double>(g * (size_t)nrr_blocks(p));
@@ -354,6 +359,7 @@ void fill_group_tables(char* h, const hb_plan* p, const GroupWs& w, const hb_sys
       put_ptr(L.sys_out, i, q.out);
     }
     put_ptr(L.sys_smaps, i, q.smaps);
+    put_ptr(L.sys_pdiag, i, cg ? q.precond : nullptr);
     put_ptr(L.sys_diag, i, q.packed_diag);
     float lam = q.lambda;
     std::memcpy(h + L.sys_lambda + 4 * i, &lam, 4);
@@ -462,10 +468,31 @@ int launch_cg_update(int kind, void (*fn)(CgState), dim3 grid, const CgState& s,
   return HB_OK;
 }
 
-// One CG iteration for a group: normal op with partials, x/r update, p update, advance.
+// z = P r for every system of the group (circulant preconditioner, identity for systems
+// without one): forward FFT, x diagonal / nv, inverse FFT, then the Re<r, z> partials
+// (and p = z at initialisation).
+int cg_precondition(const hb_plan* p, const CgState& s, dim3 ugrid, int init, cudaStream_t st) {
+  HB_CUDA(cudaMemcpyAsync(s.z, s.r, (size_t)s.nsys * s.nv * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+  const float2* tw = p->tables + p->to.total;
+  HB_CUDA(fftl::fft3_grid<-1>(p->N0, p->N1, p->N2, tw, s.z, s.nsys, st, HB_KERNEL_CG_UPDATE));
+  if (int r = launch_cg_update(HB_KERNEL_CG_UPDATE, cg_precond_scale_kernel, ugrid, s, st)) return r;
+  HB_CUDA(fftl::fft3_grid<1>(p->N0, p->N1, p->N2, tw, s.z, s.nsys, st, HB_KERNEL_CG_UPDATE));
+  {
+    LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
+    cg_rz_kernel<<<ugrid, 256, 0, st>>>(s, init);
+  }
+  HB_CHECK_LAUNCH();
+  return HB_OK;
+}
+constexpr int kKernelsPerPrecondition = 8;  // 2 x 3 FFT passes, scale, partials
+
+// One CG iteration for a group: normal op with partials, x/r update, [z = P r], p update,
+// advance.
 int cg_iteration(const hb_plan* p, const PassArgs& a, const CgState& s, dim3 ugrid, int* iter, cudaStream_t st) {
   if (int r = run_normal(p, a, st)) return r;
   if (int r = launch_cg_update(HB_KERNEL_CG_UPDATE, cg_step_xr_kernel, ugrid, s, st)) return r;
+  if (s.z)
+    if (int r = cg_precondition(p, s, ugrid, 0, st)) return r;
   if (int r = launch_cg_update(HB_KERNEL_CG_UPDATE, cg_step_p_kernel, ugrid, s, st)) return r;
   {
     LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
@@ -513,8 +540,14 @@ int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int it
     s.pap_part = w.pap; s.npap = npap_blocks(p);
     s.rr_part = w.rr;
     s.tol = tol;
+    bool precond = false;
+    for (int64_t i = 0; i < g; ++i) precond = precond || sys[s0 + i].precond != nullptr;
+    s.z = precond ? w.z : nullptr;
+    s.sys_pdiag = (const float* const*)(w.tables + w.L.sys_pdiag);
     dim3 ugrid(nrr, (unsigned)g);
     if (int r = launch_cg_update(HB_KERNEL_CG_UPDATE, cg_init_kernel, ugrid, s, st)) return r;
+    if (precond)
+      if (int r = cg_precondition(p, s, ugrid, 1, st)) return r;
     {
       LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
       cg_init_finish_kernel<<<(unsigned)g, 256, 0, st>>>(s, nrr);
@@ -559,7 +592,8 @@ int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int it
         return fail(HB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
       }
       for (int it = 0; it < iters && ce == cudaSuccess; ++it) ce = cudaGraphLaunch(exec, cs);
-      g_launches.fetch_add((uint64_t)kKernelsPerCgIteration * iters, std::memory_order_relaxed);
+      g_launches.fetch_add((uint64_t)(kKernelsPerCgIteration + (precond ? kKernelsPerPrecondition : 0)) * iters,
+                           std::memory_order_relaxed);
       cudaError_t ce2 = cudaSuccess;
       if (!own) {
         ce2 = cudaEventRecord(gs->e2, cs);
@@ -720,6 +754,10 @@ int hb_plan_create(hb_plan** out, int64_t nz, int64_t ny, int64_t nx, int device
   // twiddle tables in FP64 on the host, rounded to float
   std::vector<float2> h(p->to.total);
   fill_tables(h.data(), p->N0, p->N1, p->N2);
+  // + the team tables of nz, ny, nx (image-grid FFTs of the preconditioner)
+  const int nimg[3] = {p->N0, p->N1, p->N2};
+  const std::vector<float2> himg = fftl::team_tables(nimg);
+  h.insert(h.end(), himg.begin(), himg.end());
   cudaError_t e = cudaMalloc(&p->tables, h.size() * sizeof(float2));
   if (e == cudaSuccess) e = cudaMemcpy(p->tables, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {

@@ -7,6 +7,9 @@
 //                alpha = rz[i] / pAp;  x += alpha p;  r -= alpha Ap;  partials of Re<r,r>
 //   step_p:      rz[i+1] = sum(partials); p = r + (rz[i+1] / rz[i]) p;
 //                sqrt(rz[i+1]) < tol -> status CONVERGED
+// Preconditioned (z != null): between step_xr and step_p the host applies z = P r and
+// cg_rz replaces the partials by those of Re<r, z>; step_p then uses z for r, as
+// opalgs.cpp:78-88 does (and the tolerance test reads sqrt(Re<r, z>)).
 // Every CTA reduces the partial arrays itself in one fixed order, so all CTAs agree
 // bit for bit and no host synchronisation is needed.  A system whose status is not
 // RUNNING is skipped by every later kernel (active[sys] == 0).
@@ -36,6 +39,8 @@ struct CgState {
   int npap;
   double* rr_part;       // [nsys][gridDim.x of the update kernels]
   double tol;
+  float2* z;             // [nsys][nv] preconditioned residual (null: no preconditioner)
+  const float* const* sys_pdiag;  // [nsys] circulant preconditioner diagonals (entries nullable)
 };
 
 // Deterministic block-wide sum of n doubles (same order in every CTA).
@@ -143,8 +148,9 @@ __global__ void __launch_bounds__(256) cg_step_p_kernel(CgState s) {
   const double rzold = s.rz[(long long)sys * s.rz_ld + it];
   const float beta = (float)(rznew / rzold);
   const long long base = (long long)sys * s.nv;
+  const float2* zr = s.z ? s.z : s.r;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x) {
-    const float2 r = s.r[base + i];
+    const float2 r = zr[base + i];
     float2 p = s.p[base + i];
     p.x = fmaf(beta, p.x, r.x);
     p.y = fmaf(beta, p.y, r.y);
@@ -158,6 +164,33 @@ __global__ void __launch_bounds__(256) cg_step_p_kernel(CgState s) {
       s.active[sys] = 0;
     }
   }
+}
+
+// Partials of Re<r, z> (replacing those of Re<r, r>); at initialisation also p = z.
+__global__ void __launch_bounds__(256) cg_rz_kernel(CgState s, int init) {
+  __shared__ double red[32];
+  const int sys = blockIdx.y;
+  if (!init && !s.active[sys]) return;
+  const long long base = (long long)sys * s.nv;
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x) {
+    const float2 r = s.r[base + i];
+    const float2 z = s.z[base + i];
+    if (init) s.p[base + i] = z;
+    acc += (double)r.x * z.x + (double)r.y * z.y;
+  }
+  block_write_partial(acc, s.rr_part + (long long)sys * gridDim.x + blockIdx.x, red);
+}
+
+// Frequency-domain step of z = P r: z[sys] *= pdiag[sys] / nv (identity for a system
+// without a preconditioner; 1/nv is the inverse FFT's normalisation).
+__global__ void __launch_bounds__(256) cg_precond_scale_kernel(CgState s) {
+  const int sys = blockIdx.y;
+  const float* d = s.sys_pdiag[sys];
+  const float inv = 1.f / (float)s.nv;
+  const long long base = (long long)sys * s.nv;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x)
+    s.z[base + i] = cscale(s.z[base + i], d ? d[i] * inv : inv);
 }
 
 // Ends an iteration: every kernel of the next one reads the advanced counter.

@@ -10,11 +10,14 @@
 #include <vector>
 
 #include "../../include/hasty_b200.h"
-#include "fft3_kernels.cuh"
+#include "fft3_launch.cuh"
 #include "nufft_kernels.cuh"
 #include "runtime.cuh"
 
 using namespace hb;
+using hb::fftl::fft3_grid;
+using hb::fftl::team_length;
+using hb::fftl::team_tables;
 
 struct hb_nufft {
   int device;
@@ -30,21 +33,9 @@ struct hb_nufft {
 
 namespace {
 
-bool team_length(int L, int* E, int* S) {
-  switch (L) {
-    case 8: *E = 4; *S = 2; return true;
-    case 16: *E = 4; *S = 4; return true;
-    case 32: *E = 8; *S = 4; return true;
-    case 64: *E = 8; *S = 8; return true;
-    case 128: *E = 16; *S = 8; return true;
-    case 256: *E = 16; *S = 16; return true;
-    case 96: *E = 24; *S = 4; return true;
-    case 160: *E = 40; *S = 4; return true;
-    case 192: *E = 24; *S = 8; return true;
-    case 320: *E = 40; *S = 8; return true;
-    case 512: *E = 32; *S = 16; return true;
-    default: return false;
-  }
+template <int DIR>
+cudaError_t fft3(const hb_nufft* p, float2* grid, int nt, cudaStream_t st) {
+  return fft3_grid<DIR>(p->g.n[0], p->g.n[1], p->g.n[2], p->tw, grid, nt, st);
 }
 
 // Kernel width for a requested tolerance (upsampling 2): w = ceil(log10(1/tol)) + 1.
@@ -66,112 +57,6 @@ double phi_hat(int k, int n, int w, double beta) {
   double acc = f(0.0) + f(hw);
   for (int i = 1; i < M; ++i) acc += (i & 1 ? 4.0 : 2.0) * f(i * h);
   return 2.0 * acc * h / 3.0;  // even integrand: twice the half-interval
-}
-
-// ---- 3D FFT of nt grids [n0][n1][n2], in place ----
-template <auto kernel>
-cudaError_t allow_smem(size_t bytes) {
-  static bool done[64] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || done[dev & 63] || bytes <= 48 * 1024) return e;
-  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess) done[dev & 63] = true;
-  return e;
-}
-
-template <int L, int DIR>
-cudaError_t lines_contig(float2* d, long long nlines, const float2* tw, cudaStream_t st) {
-  using C = LineCfg<L>;
-  const size_t smem = C::SMEM_C * sizeof(float2);
-  cudaError_t e = allow_smem<fft_lines_contig_kernel<L, DIR>>(smem);
-  if (e != cudaSuccess) return e;
-  long long blocks = (nlines + C::NTEAMS_C - 1) / C::NTEAMS_C;
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  LaunchScope ls(HB_KERNEL_NUFFT, st);
-  fft_lines_contig_kernel<L, DIR><<<(unsigned)blocks, C::THREADS_C, smem, st>>>(d, nlines, tw);
-  return cudaGetLastError();
-}
-
-template <int L, int DIR>
-cudaError_t lines_strided(float2* d, long long row_stride, int ncols, int ny, long long oy, int nz, long long oz,
-                          const float2* tw, cudaStream_t st) {
-  using C = LineCfg<L>;
-  const size_t smem = C::SMEM_S * sizeof(float2);
-  cudaError_t e = allow_smem<fft_lines_strided_kernel<L, DIR>>(smem);
-  if (e != cudaSuccess) return e;
-  dim3 grid((ncols + C::XT - 1) / C::XT, ny, nz);
-  LaunchScope ls(HB_KERNEL_NUFFT, st);
-  fft_lines_strided_kernel<L, DIR><<<grid, C::THREADS_S, smem, st>>>(d, row_stride, ncols, oy, oz, tw);
-  return cudaGetLastError();
-}
-
-template <int DIR>
-cudaError_t contig_any(int L, float2* d, long long nlines, const float2* tw, cudaStream_t st) {
-  switch (L) {
-    case 8: return lines_contig<8, DIR>(d, nlines, tw, st);
-    case 16: return lines_contig<16, DIR>(d, nlines, tw, st);
-    case 32: return lines_contig<32, DIR>(d, nlines, tw, st);
-    case 64: return lines_contig<64, DIR>(d, nlines, tw, st);
-    case 128: return lines_contig<128, DIR>(d, nlines, tw, st);
-    case 256: return lines_contig<256, DIR>(d, nlines, tw, st);
-    case 96: return lines_contig<96, DIR>(d, nlines, tw, st);
-    case 160: return lines_contig<160, DIR>(d, nlines, tw, st);
-    case 192: return lines_contig<192, DIR>(d, nlines, tw, st);
-    case 320: return lines_contig<320, DIR>(d, nlines, tw, st);
-    case 512: return lines_contig<512, DIR>(d, nlines, tw, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-template <int DIR>
-cudaError_t strided_any(int L, float2* d, long long rs, int ncols, int ny, long long oy, int nz, long long oz,
-                        const float2* tw, cudaStream_t st) {
-  switch (L) {
-    case 8: return lines_strided<8, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 16: return lines_strided<16, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 32: return lines_strided<32, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 64: return lines_strided<64, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 128: return lines_strided<128, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 256: return lines_strided<256, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 96: return lines_strided<96, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 160: return lines_strided<160, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 192: return lines_strided<192, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 320: return lines_strided<320, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    case 512: return lines_strided<512, DIR>(d, rs, ncols, ny, oy, nz, oz, tw, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-// nt grids [n0][n1][n2] in place; tw: team tables of n0, n1, n2 back to back
-template <int DIR>
-cudaError_t fft3_grid(int n0, int n1, int n2, const float2* tw, float2* grid, int nt, cudaStream_t st) {
-  const long long vol = (long long)n0 * n1 * n2;
-  cudaError_t e = contig_any<DIR>(n2, grid, (long long)nt * n0 * n1, tw + n0 + n1, st);
-  if (e != cudaSuccess) return e;
-  e = strided_any<DIR>(n1, grid, n2, n2, n0, (long long)n1 * n2, nt, vol, tw + n0, st);
-  if (e != cudaSuccess) return e;
-  return strided_any<DIR>(n0, grid, (long long)n1 * n2, n2, n1, n2, nt, vol, tw, st);
-}
-
-template <int DIR>
-cudaError_t fft3(const hb_nufft* p, float2* grid, int nt, cudaStream_t st) {
-  return fft3_grid<DIR>(p->g.n[0], p->g.n[1], p->g.n[2], p->tw, grid, nt, st);
-}
-
-// Team twiddle tables of the three lengths, back to back (forward sign, FP64 rounded).
-std::vector<float2> team_tables(const int* n) {
-  std::vector<float2> tw;
-  for (int a = 0; a < 3; ++a) {
-    int E = 0, S = 0;
-    team_length(n[a], &E, &S);
-    for (int k1 = 0; k1 < E; ++k1)
-      for (int t = 0; t < S; ++t) {
-        const double ang = -2.0 * M_PI * (double)(t * k1) / (double)n[a];
-        tw.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
-      }
-  }
-  return tw;
 }
 
 template <int W>
@@ -254,6 +139,43 @@ void free_plan(hb_nufft* p) {
 }
 
 }  // namespace
+
+namespace hb {
+
+int nufft_psf_circulant(const int* M, const float* coords, int64_t nsamples, double tol, int device, float2* out,
+                        cudaStream_t st) {
+  const long long vol = (long long)M[0] * M[1] * M[2];
+  hb_nufft* np = nullptr;
+  // type 1 over the grid's modes: sum_j exp(+i c_j . d), d in [-M/2, M/2)
+  if (int r = hb_nufft_create(&np, M[0], M[1], M[2], coords, nsamples, tol, 1, device, st)) return r;
+  float2* ones = nullptr;
+  int rc = HB_OK;
+  cudaError_t e = cudaMalloc(&ones, nsamples * sizeof(float2));
+  if (e == cudaSuccess) {
+    {
+      LaunchScope ls(HB_KERNEL_DIAG, st);
+      fill_c64_kernel<<<(unsigned)((nsamples + 255) / 256), 256, 0, st>>>(ones, nsamples, make_float2(1.f, 0.f));
+    }
+    rc = type1_batch(np, ones, nsamples, np->modes, vol, 1, +1, st);
+    if (rc == HB_OK) {
+      LaunchScope ls(HB_KERNEL_DIAG, st);
+      ifftshift3_scale_kernel<<<(unsigned)((vol + 255) / 256), 256, 0, st>>>(np->modes, M[0], M[1], M[2],
+                                                                             (float)(1.0 / (double)vol), out);
+    }
+    if (rc == HB_OK && (e = cudaGetLastError()) != cudaSuccess)
+      rc = fail(HB_ERR_CUDA, std::string("psf: ") + cudaGetErrorString(e));
+    if (rc == HB_OK && (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      rc = fail(HB_ERR_CUDA, std::string("psf: ") + cudaGetErrorString(e));
+  } else {
+    rc = fail(HB_ERR_CUDA, std::string("psf: ") + cudaGetErrorString(e));
+  }
+  if (rc != HB_OK) cudaStreamSynchronize(st);
+  cudaFree(ones);
+  hb_nufft_destroy(np);
+  return rc;
+}
+
+}  // namespace hb
 
 extern "C" {
 
@@ -441,19 +363,15 @@ int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsampl
   cudaStream_t st = (cudaStream_t)stream;
   const int M[3] = {2 * N[0], 2 * N[1], 2 * N[2]};
   const long long vol = (long long)M[0] * M[1] * M[2];
-  hb_nufft* np = nullptr;
-  // type 1 over the 2x grid's modes: psf(d) = sum_j exp(+i c_j . d), d in [-N, N)
-  if (int r = hb_nufft_create(&np, M[0], M[1], M[2], coords, nsamples, tol, 1, dev, stream)) return r;
-  float2* ones = nullptr;
+  float2* T = nullptr;
   float2* tw = nullptr;
   int rc = HB_OK;
   auto cuda_fail = [&](cudaError_t e, const char* what) {
     rc = fail(HB_ERR_CUDA, std::string("hb_diag_build_nufft: ") + what + ": " + cudaGetErrorString(e));
-    return rc;
   };
   do {
     cudaError_t e;
-    if ((e = cudaMalloc(&ones, nsamples * sizeof(float2))) != cudaSuccess) { cuda_fail(e, "alloc"); break; }
+    if ((e = cudaMalloc(&T, vol * sizeof(float2))) != cudaSuccess) { cuda_fail(e, "alloc"); break; }
     const std::vector<float2> tables = team_tables(M);
     if ((e = cudaMalloc(&tw, tables.size() * sizeof(float2))) != cudaSuccess) { cuda_fail(e, "alloc"); break; }
     if ((e = cudaMemcpyAsync(tw, tables.data(), tables.size() * sizeof(float2), cudaMemcpyHostToDevice, st)) !=
@@ -461,19 +379,8 @@ int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsampl
       cuda_fail(e, "upload");
       break;
     }
-    {
-      LaunchScope ls(HB_KERNEL_DIAG, st);
-      fill_c64_kernel<<<(unsigned)((nsamples + 255) / 256), 256, 0, st>>>(ones, nsamples, make_float2(1.f, 0.f));
-    }
-    if ((rc = type1_batch(np, ones, nsamples, np->modes, vol, 1, +1, st)) != HB_OK) break;
-    // the fine grid is free again: T in circulant layout there, then the forward FFT
-    float2* T = np->grid;
-    {
-      LaunchScope ls(HB_KERNEL_DIAG, st);
-      ifftshift3_scale_kernel<<<(unsigned)((vol + 255) / 256), 256, 0, st>>>(np->modes, M[0], M[1], M[2],
-                                                                             (float)(1.0 / (double)vol), T);
-    }
-    if ((e = cudaGetLastError()) != cudaSuccess) { cuda_fail(e, "kernel launch"); break; }
+    // PSF in circulant layout on the 2x grid, then T = FFT(PSF)
+    if ((rc = nufft_psf_circulant(M, coords, nsamples, tol, dev, T, st)) != HB_OK) break;
     if ((e = fft3_grid<-1>(M[0], M[1], M[2], tw, T, 1, st)) != cudaSuccess) { cuda_fail(e, "fft"); break; }
     if (packed && (rc = hb_diag_pack(plan, T, packed, stream)) != HB_OK) break;
     if (T_complex &&
@@ -484,9 +391,8 @@ int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsampl
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) cuda_fail(e, "sync");
   } while (false);
   if (rc != HB_OK) cudaStreamSynchronize(st);
-  cudaFree(ones);
+  cudaFree(T);
   cudaFree(tw);
-  hb_nufft_destroy(np);
   return rc;
 }
 

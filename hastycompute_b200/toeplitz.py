@@ -49,10 +49,12 @@ class System:
     x: image [nz, ny, nx] (CG: initial guess, overwritten with the solution); out: the
     normal-op output; b: CG right-hand side; smaps: this system's coil maps; coils:
     indices into them (default all); packed: this system's packed diagonal (1-D view);
-    lam: adds lam * x."""
+    lam: adds lam * x; precond: CG only, a circulant preconditioner from
+    ``ToeplitzPlan.build_preconditioner`` (preconditioned CG for this system)."""
 
-    def __init__(self, x, smaps, packed, out=None, b=None, coils=None, lam=0.0):
+    def __init__(self, x, smaps, packed, out=None, b=None, coils=None, lam=0.0, precond=None):
         self.x, self.out, self.b, self.smaps, self.packed, self.lam = x, out, b, smaps, packed, float(lam)
+        self.precond = precond
         self.coils = list(range(smaps.shape[0])) if coils is None else [int(c) for c in coils]
 
 
@@ -252,6 +254,39 @@ class ToeplitzPlan:
         capi.check(code)
         return list(status), list(done)
 
+    # ------------------------------------------------------ circulant preconditioner ----
+    def numel(self):
+        n0, n1, n2 = self.shape
+        return n0 * n1 * n2
+
+    def build_preconditioner(self, coords, smaps, coils=None, lam=0.0, tol=1e-6):
+        """Circulant preconditioner (``CirculantPreconditionerOp::build_diagonal``,
+        ``lib/mri/precond.cpp:65-117``; ``torch_precond.py:60-105``) of sum_c S_c^H A^H A S_c
+        + lam I for a trajectory coords [3, K] float32: float32 [nz, ny, nx] in FFT order."""
+        if coords.dtype != torch.float32 or coords.dim() != 2 or coords.shape[0] != 3:
+            raise RuntimeError("coords must be float32 [3, K]")
+        coords = coords.to(self.device).contiguous()
+        _check_c64(smaps, "smaps", self.device, self.shape)
+        coils = list(range(smaps.shape[0])) if coils is None else [int(c) for c in coils]
+        if not coils or any(c < 0 or c >= smaps.shape[0] for c in coils):
+            raise RuntimeError("coil index out of range")
+        out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        capi.check(self.lib.hb_precond_build(self._h, _ptr(coords), coords.shape[1], float(tol), _ptr(smaps),
+                                             capi.i64_array(coils), len(coils), float(lam), _ptr(out),
+                                             _stream_ptr(self.device)))
+        return out
+
+    def apply_preconditioner(self, precond, x, out=None):
+        """out = P x = IFFT(precond * FFT(x)) (``CirculantPreconditionerOp::apply``, precond.cpp:30-52)."""
+        _check_c64(x, "x", self.device, self.shape)
+        if out is None:
+            out = torch.empty_like(x)
+        _check_c64(out, "out", self.device, self.shape)
+        if precond.dtype != torch.float32 or precond.numel() != self.numel() or not precond.is_contiguous():
+            raise RuntimeError("precond must be a contiguous float32 [nz, ny, nx] tensor")
+        capi.check(self.lib.hb_precond_apply(self._h, _ptr(precond), _ptr(x), _ptr(out), _stream_ptr(self.device)))
+        return out
+
     # ------------------------------------------------------- heterogeneous batch ----
     def _systems(self, systems, cg):
         arr = (capi.HbSystem * len(systems))()
@@ -278,6 +313,14 @@ class ToeplitzPlan:
             arr[i].ncoil = len(q.coils)
             arr[i].packed_diag = q.packed.data_ptr()
             arr[i].lam = q.lam
+            pc = getattr(q, "precond", None)
+            if pc is not None:
+                if not cg:
+                    raise RuntimeError("a preconditioner only applies to CG systems")
+                if pc.dtype != torch.float32 or pc.numel() != self.numel() or not pc.is_contiguous() or \
+                        pc.device != self.device:
+                    raise RuntimeError("precond must be a contiguous float32 [nz, ny, nx] tensor on the device")
+                arr[i].precond = pc.data_ptr()
         return arr, keep
 
     def sense_normal_systems(self, systems, workspace_bytes=None):

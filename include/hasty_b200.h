@@ -127,6 +127,10 @@ typedef struct hb_system {
   int64_t ncoil;
   const float* packed_diag;
   float lambda;
+  /* CG only, nullable: circulant preconditioner of this system ([nz][ny][nx] float32 from
+   * hb_precond_build); when set, hb_cg_run_systems runs preconditioned CG for it
+   * (opalgs.cpp:50-96 with P).  Zero-initialise the struct to leave it unset. */
+  const float* precond;
 } hb_system;
 
 /* Workspace bytes for nsys systems with total_coils (system, coil) pairs handled in one
@@ -245,6 +249,23 @@ int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsampl
 /* SENSE forward: kdata[b] = type2(S[coils[b]] * x) (isign -1). */
 int hb_sense_forward_nufft(const hb_nufft* plan, const void* x, const void* smaps, const int64_t* coils,
                            int64_t ncoil, void* kdata, void* stream);
+
+/* ---- Circulant preconditioner ----
+ *
+ * Replaces hasty::mri::CirculantPreconditionerOp (build_diagonal and apply,
+ * lib/mri/precond.cpp:17-117) and circulant_precond (python/python/hastypy/base/
+ * torch_precond.py:60-105).  P = IFFT diag(precond) FFT on the nz x ny x nx grid, the
+ * inverse of the best circulant approximation of sum_c S_c^H A^H A S_c + lambda I (the
+ * operator hb_cg_run_systems solves): precond[k] = 1 / (d[k] + lambda) with d[k] its
+ * Fourier-domain diagonal, evaluated from the trajectory's PSF (a type-1 NUFFT at `tol`)
+ * and the coil maps' autocorrelations on the 2x grid.  precond is float32 [nz][ny][nx] in
+ * FFT (uncentred) order.  hb_precond_build allocates its temporaries for the duration of
+ * the call (a NUFFT fine grid of (4nz)(4ny)(4nx) complex64, then up to nine (2nz)(2ny)(2nx)
+ * arrays) and synchronises `stream`.  `coils` is a HOST array of ncoil map indices. */
+int hb_precond_build(const hb_plan* plan, const float* coords, int64_t nsamples, double tol, const void* smaps,
+                     const int64_t* coils, int64_t ncoil, float lambda, float* precond, void* stream);
+/* out = P in (one image; in == out allowed). */
+int hb_precond_apply(const hb_plan* plan, const float* precond, const void* in, void* out, void* stream);
 
 /* ---- measurement hooks (no counterpart in the reference; used by benchmarks) ----
  * Kernel kinds for the profile counters. */

@@ -24,6 +24,8 @@ LibTorch).  File references below are paths inside the reference project:
   (``python/python/hastypy/base/torch_opalg.py:49-61``).
 * ``lib/fft/nufft.cpp:540-767`` the type-1 / type-2 NUFFTs of ``CUDANufft`` and the SENSE
   forward / adjoint around them (``lib/mri/sense.ixx:426-497``), as direct NUDFTs.
+* ``lib/mri/precond.cpp:65-117`` the circulant preconditioner (the Fourier-domain diagonal of
+  the SENSE normal operator, inverted) and its apply.
 * ``lib/fft/nufft.cpp:410-767`` / ``:785-920`` explicit NUFFT normal op on the N grid
   (type-2 then type-1, each /sqrt(prod(N))), evaluated as a dense direct NUDFT.
   ``Toeplitz = explicit / 2^3`` in 3D because of the two different grid scalings.
@@ -160,6 +162,31 @@ def sense_forward(coords, x, smaps, coils=None):
     smaps = np.asarray(smaps, np.complex128)
     coils = range(smaps.shape[0]) if coils is None else coils
     return nudft_type2(coords, np.stack([smaps[c] * x for c in coils]), -1)
+
+
+def circulant_precond(coords, smaps, lam=0.0, coils=None):
+    """Circulant preconditioner (``CirculantPreconditionerOp::build_diagonal``,
+    ``lib/mri/precond.cpp:65-117``; ``torch_precond.py:60-105``, both ported from sigpy):
+    1 / (d + lam) with d[k] = (F B F^H)[k, k] the Fourier-domain diagonal of
+    B = sum_c S_c^H Top S_c, in FFT (uncentred) order, float64:
+    d = FFT_2N(psf * IFFT_2N(sum_c |FFT_2N(pad(conj S_c))|^2))[::2, ::2, ::2] / prod(N)."""
+    smaps = np.asarray(smaps, np.complex128)
+    coils = range(smaps.shape[0]) if coils is None else coils
+    N = smaps.shape[1:]
+    M = grid2(N)
+    psf = psf_circulant(coords, N)
+    q = 0.0
+    for c in coils:
+        q = q + np.abs(np.fft.fftn(np.conj(smaps[c]), s=M, axes=(0, 1, 2))) ** 2
+    g = psf * np.fft.ifftn(q)
+    d = np.fft.fftn(g)[::2, ::2, ::2].real / float(np.prod(N)) + lam
+    return np.where(d > 0, 1.0 / np.where(d > 0, d, 1.0), 1.0)
+
+
+def precond_apply(P, x):
+    """``CirculantPreconditionerOp::apply`` (``precond.cpp:30-52``) in FFT order:
+    IFFT(P * FFT(x))."""
+    return np.fft.ifftn(P * np.fft.fftn(np.asarray(x, np.complex128)))
 
 
 def vdot(a, b):

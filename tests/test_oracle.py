@@ -149,3 +149,28 @@ def test_sense_adjoint_forward_oracle_pair():
     lhs = np.vdot(O.sense_forward(c, x, sm, coils).ravel(), kd.ravel())
     rhs = np.vdot(x.ravel(), O.sense_adjoint(c, kd, sm, coils).ravel())
     assert abs(lhs - rhs) < 1e-10 * abs(rhs)
+
+
+def test_circulant_precond_is_the_fourier_diagonal():
+    """The preconditioner's d[k] equals the diagonal of F B F^H (F the unitary DFT of the
+    N grid, B = sum_c S_c^H Top S_c + lam I), computed here by brute force column by
+    column; and P is Hermitian positive definite."""
+    rng = np.random.default_rng(7)
+    shape, K, lam = (4, 3, 5), 60, 0.3
+    c = rng.uniform(-np.pi, np.pi, (3, K))
+    sm = rng.standard_normal((2,) + shape) + 1j * rng.standard_normal((2,) + shape)
+    T = O.toeplitz_diagonal(c, shape)
+    n = int(np.prod(shape))
+    d_brute = np.empty(n)
+    for k in range(n):
+        e = np.zeros(n, np.complex128)
+        e[k] = 1.0
+        fk = np.fft.ifftn(e.reshape(shape), norm="ortho")  # F^H e_k
+        Bf = O.sense_normal_toeplitz(fk, sm, T) + lam * fk
+        d_brute[k] = np.fft.fftn(Bf, norm="ortho").ravel()[k].real  # (F B F^H)[k, k]
+    P = O.circulant_precond(c, sm, lam)
+    assert np.allclose(1.0 / P.ravel(), d_brute, rtol=1e-10, atol=1e-12)
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    y = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    assert abs(O.vdot(y, O.precond_apply(P, x)) - O.vdot(O.precond_apply(P, y), x)) < 1e-12
+    assert O.vdot(x, O.precond_apply(P, x)).real > 0
