@@ -29,6 +29,7 @@ struct hb_nufft {
   float2* tw = nullptr;     // team twiddle tables of n0, n1, n2 (offsets 0, n0, n0 + n1)
   float2* grid = nullptr;   // [maxbatch][n0][n1][n2]
   float2* modes = nullptr;  // [maxbatch][N0][N1][N2] (SENSE temporaries)
+  float2* kbuf = nullptr;   // [maxbatch][K] (SENSE normal temporaries)
 };
 
 namespace {
@@ -135,6 +136,7 @@ void free_plan(hb_nufft* p) {
   cudaFree(p->tw);
   cudaFree(p->grid);
   cudaFree(p->modes);
+  cudaFree(p->kbuf);
   delete p;
 }
 
@@ -229,6 +231,7 @@ int hb_nufft_create(hb_nufft** out, int64_t nz, int64_t ny, int64_t nx, const fl
   if ((e = cudaMalloc(&p->tw, (g.n[0] + g.n[1] + g.n[2]) * sizeof(float2))) != cudaSuccess) return bail(e, "tables");
   if ((e = cudaMalloc(&p->grid, (size_t)maxbatch * vol * sizeof(float2))) != cudaSuccess) return bail(e, "fine grid");
   if ((e = cudaMalloc(&p->modes, (size_t)maxbatch * nm * sizeof(float2))) != cudaSuccess) return bail(e, "modes");
+  if ((e = cudaMalloc(&p->kbuf, (size_t)maxbatch * nsamples * sizeof(float2))) != cudaSuccess) return bail(e, "kbuf");
   if ((e = cudaMalloc(&bin_of, nsamples * sizeof(int))) != cudaSuccess) return bail(e, "bins");
   if ((e = cudaMalloc(&counts, 2 * nbins * sizeof(int))) != cudaSuccess) return bail(e, "bins");
 
@@ -349,6 +352,47 @@ int hb_sense_forward_nufft(const hb_nufft* plan, const void* x, const void* smap
     }
     HB_CHECK_LAUNCH();
     if (int r = type2_batch(plan, plan->modes, nm, (float2*)kdata + b0 * K, K, nb, -1, st)) return r;
+  }
+  return HB_OK;
+}
+
+int hb_sense_normal_nufft(const hb_nufft* plan, const void* x, const void* smaps, const int64_t* coils, int64_t ncoil,
+                          const void* kdata, const float* weights, void* out, int accumulate, void* stream) {
+  if (!plan || !x || !smaps || !out || ncoil < 0 || (ncoil > 0 && !coils))
+    return fail(HB_ERR_INVALID, "hb_sense_normal_nufft: null argument or negative ncoil");
+  for (int64_t b = 0; b < ncoil; ++b)
+    if (coils[b] < 0) return fail(HB_ERR_INVALID, "hb_sense_normal_nufft: negative coil index");
+  DeviceGuard dg(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long K = plan->g.K, nm = nmodes(plan);
+  const unsigned vb = (unsigned)((nm + 255) / 256), kb = (unsigned)((K + 255) / 256);
+  if (ncoil == 0 && !accumulate) HB_CUDA(cudaMemsetAsync(out, 0, nm * sizeof(float2), st));
+  for (int64_t b0 = 0; b0 < ncoil; b0 += plan->maxbatch) {
+    const int nb = (int)((ncoil - b0) < plan->maxbatch ? (ncoil - b0) : plan->maxbatch);
+    CoilMaps maps{};
+    KdataPtrs ys{};
+    for (int b = 0; b < nb; ++b) {
+      maps.s[b] = (const float2*)smaps + coils[b0 + b] * nm;
+      ys.y[b] = kdata ? (const float2*)kdata + coils[b0 + b] * K : nullptr;
+    }
+    {
+      LaunchScope ls(HB_KERNEL_NUFFT, st);
+      sense_coil_expand_kernel<<<vb, 256, 0, st>>>((const float2*)x, nb, nm, maps, plan->modes);
+    }
+    HB_CHECK_LAUNCH();
+    if (int r = type2_batch(plan, plan->modes, nm, plan->kbuf, K, nb, -1, st)) return r;
+    if (kdata || weights) {
+      LaunchScope ls(HB_KERNEL_NUFFT, st);
+      sense_kspace_mid_kernel<<<kb, 256, 0, st>>>(plan->kbuf, nb, K, ys, weights);
+    }
+    HB_CHECK_LAUNCH();
+    if (int r = type1_batch(plan, plan->kbuf, K, plan->modes, nm, nb, +1, st)) return r;
+    {
+      LaunchScope ls(HB_KERNEL_NUFFT, st);
+      sense_coil_combine_kernel<<<vb, 256, 0, st>>>(plan->modes, nb, nm, maps, (float2*)out,
+                                                    (b0 > 0 || accumulate) ? 1 : 0);
+    }
+    HB_CHECK_LAUNCH();
   }
   return HB_OK;
 }

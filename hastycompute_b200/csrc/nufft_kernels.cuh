@@ -239,6 +239,22 @@ __global__ void sense_coil_combine_kernel(const float2* f, int nb, long long nvo
   out[v] = acc;
 }
 
+// k-space step of the SENSE normal operator (the reference's mid-appliers):
+// k[b][j] = (k[b][j] - y_b[j]) * w[j]  (y_b and w nullable)
+struct KdataPtrs {
+  const float2* y[kNufftMaxBatch];
+};
+__global__ void sense_kspace_mid_kernel(float2* k, int nb, long long K, KdataPtrs y, const float* w) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= K) return;
+  const float wj = w ? w[j] : 1.f;
+  for (int b = 0; b < nb; ++b) {
+    float2 v = k[b * K + j];
+    if (y.y[b]) v = csub(v, y.y[b][j]);
+    k[b * K + j] = cscale(v, wj);
+  }
+}
+
 // f[b] = S_b * x
 __global__ void sense_coil_expand_kernel(const float2* x, int nb, long long nvox, CoilMaps maps, float2* f) {
   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;

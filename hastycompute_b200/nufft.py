@@ -7,12 +7,13 @@ Mirrors the reference's NUFFT front end:
 * ``CUDANufft(coords, nmodes, opts).apply(in, out)`` -- ``nufft.ixx:108-160`` /
   ``nufft.cpp:540-767`` with ``nmodes = [ntransf, nz, ny, nx]``: type 1 maps
   ``in [ntransf, nfreq]`` to ``out [ntransf, nz, ny, nx]``, type 2 the reverse;
-* ``NufftPlan.sense_adjoint`` / ``sense_forward`` -- the coil loops of the SENSE operators
-  built on those plans (``lib/mri/sense.ixx:426-497``); ``sense_adjoint`` gives the CG
+* ``NufftPlan.sense_adjoint`` / ``sense_forward`` / ``sense_normal`` -- the coil loops of the
+  SENSE operators built on those plans (``lib/mri/sense.ixx:426-497``), the normal one with
+  the k-space manipulators of ``batch_sense.cpp:452-486``; ``sense_adjoint`` gives the CG
   right-hand side ``b = sum_c conj(S_c) NUFFT^H(y_c)``.
 
 Only 3-D transforms are compiled (the path's images are 3-D); ``2 * N`` per axis must be
-one of 8, 16, 32, 64, 128, 256, 96, 160, 192, 320.  Every call runs the sm_100a kernels of
+one of 8, 16, 32, 64, 128, 256, 512, 96, 160, 192, 320.  Every call runs the sm_100a kernels of
 ``libhasty_b200.so``; there is no fallback.
 """
 from __future__ import annotations
@@ -118,6 +119,33 @@ class NufftPlan:
         arr = (ctypes.c_int64 * max(1, len(coils)))(*coils)
         capi.check(self.lib.hb_sense_adjoint_nufft(self._h, _ptr(kdata), _ptr(smaps), arr, len(coils), _ptr(out),
                                                    1 if accumulate else 0, _stream_ptr(self.device)))
+        return out
+
+    def sense_normal(self, x, smaps, coils=None, kdata=None, weights=None, out=None, accumulate=False):
+        """out (+)= sum_b conj(S[c_b]) type1(w * (type2(S[c_b] x) - kdata[c_b])) -- the normal
+        operator with the reference's k-space manipulators (``batch_sense.cpp:452-486``);
+        kdata [C, nfreq] indexed by coil number, weights [nfreq] float32, both optional."""
+        coils = list(range(smaps.shape[0])) if coils is None else [int(c) for c in coils]
+        _check_c64(x, "x", self.device, self.shape)
+        _check_c64(smaps, "smaps", self.device, self.shape)
+        if kdata is not None:
+            kdata = kdata.reshape(-1, self.nfreq)
+            _check_c64(kdata, "kdata", self.device)
+            if kdata.shape[0] <= max(coils):
+                raise RuntimeError("kdata must hold a row for every coil index")
+        if weights is not None:
+            weights = weights.reshape(-1)
+            if weights.dtype != torch.float32 or weights.numel() != self.nfreq or weights.device != self.device \
+                    or not weights.is_contiguous():
+                raise RuntimeError("weights must be a contiguous float32 [nfreq] tensor on the device")
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.complex64, device=self.device)
+            accumulate = False
+        _check_c64(out, "out", self.device, self.shape)
+        arr = (ctypes.c_int64 * max(1, len(coils)))(*coils)
+        capi.check(self.lib.hb_sense_normal_nufft(self._h, _ptr(x), _ptr(smaps), arr, len(coils), _ptr(kdata),
+                                                  _ptr(weights), _ptr(out), 1 if accumulate else 0,
+                                                  _stream_ptr(self.device)))
         return out
 
     def sense_forward(self, x, smaps, coils=None, kdata=None):

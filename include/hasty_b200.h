@@ -218,7 +218,7 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
  * Type 1 accumulates with atomics, so its last bits vary from run to run.
  *
  * hb_nufft_create copies coords, sorts the samples by fine-grid bin and allocates the
- * fine grids of `maxbatch` (1..32) transforms plus as many mode arrays; it synchronises
+ * fine grids of `maxbatch` (1..32) transforms plus as many mode and k-space arrays; it synchronises
  * `stream`.  Transforms run in batches of maxbatch.  c is [ntransf][nsamples], f is
  * [ntransf][nz][ny][nx]. */
 typedef struct hb_nufft hb_nufft;
@@ -236,6 +236,16 @@ int hb_nufft_type2(const hb_nufft* plan, const void* f, void* c, int64_t ntransf
  * reconstructions. */
 int hb_sense_adjoint_nufft(const hb_nufft* plan, const void* kdata, const void* smaps, const int64_t* coils,
                            int64_t ncoil, void* out, int accumulate, void* stream);
+/* SENSE normal operator through the NUFFT with the reference's k-space manipulators
+ * (BatchedSenseNormal standard_kdata / standard_weighted / standard_weighted_kdata
+ * manipulators, lib/mri/batch_sense.cpp:452-486; the coil loop of sense.ixx:426-497):
+ *   out (+)= sum_b conj(S[c_b]) * type1( w * (type2(S[c_b] * x) - kdata[c_b]) ),  c_b = coils[b]
+ * kdata [C][nsamples] indexed by coil number (nullable), weights [nsamples] float32
+ * (nullable); with both NULL it is the explicit normal operator A^H A.  The plan's mode
+ * and k-space arrays are its temporaries. */
+int hb_sense_normal_nufft(const hb_nufft* plan, const void* x, const void* smaps, const int64_t* coils, int64_t ncoil,
+                          const void* kdata, const float* weights, void* out, int accumulate, void* stream);
+
 /* Toeplitz diagonal through the NUFFT, the reference's own construction
  * (build_diagonal_base, lib/fft/nufft.cpp:932-971, at tolerance `tol`): the PSF is a
  * type-1 NUFFT of unit weights onto the 2x grid's modes, shifted to circulant layout and

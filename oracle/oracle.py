@@ -164,6 +164,19 @@ def sense_forward(coords, x, smaps, coils=None):
     return nudft_type2(coords, np.stack([smaps[c] * x for c in coils]), -1)
 
 
+def sense_normal_nufft(coords, x, smaps, coils=None, kdata=None, weights=None):
+    """NUFFT SENSE normal operator with the reference's k-space manipulators
+    (``lib/mri/batch_sense.cpp:452-486``): sum_b conj(S_cb) type1(w * (type2(S_cb x) - kdata[cb]))."""
+    smaps = np.asarray(smaps, np.complex128)
+    coils = list(range(smaps.shape[0])) if coils is None else list(coils)
+    k = sense_forward(coords, x, smaps, coils)
+    if kdata is not None:
+        k = k - np.asarray(kdata, np.complex128)[coils]
+    if weights is not None:
+        k = k * np.asarray(weights, np.float64)[None]
+    return sense_adjoint(coords, k, smaps, coils)
+
+
 def circulant_precond(coords, smaps, lam=0.0, coils=None):
     """Circulant preconditioner (``CirculantPreconditionerOp::build_diagonal``,
     ``lib/mri/precond.cpp:65-117``; ``torch_precond.py:60-105``, both ported from sigpy):
