@@ -25,7 +25,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",
 ]
 
-CAPI_SOURCES = ["capi.cu", "nufft.cu", "precond.cu"]
+CAPI_SOURCES = ["capi.cu", "nufft.cu", "precond.cu", "svt.cu"]
 
 
 def _nvcc():

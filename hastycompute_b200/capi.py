@@ -87,6 +87,9 @@ SIGNATURES = {
     "hb_precond_build": (c_int, [c_void_p, c_void_p, c_i64, c_double, c_void_p, P_i64, c_i64, c_float, c_void_p,
                                  c_void_p]),
     "hb_precond_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "hb_svt_blocks": (c_int, [c_void_p, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64, c_void_p, c_i64,
+                              c_double, c_int, c_void_p]),
+    "hb_admm_vectors": (c_int, [c_i64, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_void_p]),
     "hb_launch_count": (ctypes.c_uint64, []),
     "hb_profile_start": (c_int, []),
     "hb_profile_stop": (c_int, [ctypes.POINTER(c_double), P_i64, c_int]),

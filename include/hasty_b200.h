@@ -277,6 +277,27 @@ int hb_precond_build(const hb_plan* plan, const float* coords, int64_t nsamples,
 /* out = P in (one image; in == out allowed). */
 int hb_precond_apply(const hb_plan* plan, const float* precond, const void* in, void* out, void* stream);
 
+/* ---- Locally low rank: block singular-value thresholding and ADMM vector steps ----
+ *
+ * hb_svt_blocks replaces hasty::svt::svt_soft / svt_hard on extracted blocks and the block
+ * loops of Random3DBlocksSVT / Normal3DBlocksSVT (lib/op/svt.cpp:60-490).  x is
+ * [d0][d1][S0][S1][S2] complex64 (d0 <= 32: the low-rank axis, e.g. frames; d1 e.g.
+ * encodings), thresholded in place.  corners is a DEVICE int32 [nblocks][3] array of block
+ * corners in (S0, S1, S2); a block is the matrix [d1*b0*b1*b2][d0] (extract_block with
+ * flatten_split 0 and transpose, svt.cpp:11-58).  soft = 1: singular values s -> max(s -
+ * thresh, 0); soft = 0: keep the round(thresh) largest.  The blocks of one call must not
+ * overlap (they are processed concurrently); a corner whose block does not fit is
+ * skipped.  Singular values come from an FP64 eigen-decomposition of the block's Gram
+ * matrix (cyclic Jacobi), the block update is in FP32.
+ *
+ * hb_admm_vectors: the scaled-ADMM vector steps around the CG x-update and the SVT
+ * z-update (opalgs.cpp:103-111, batch_sense.ixx:302-431), n complex64 values:
+ *   stage 0: b = b0 + (rho/2)(z - u);  stage 1: z = x + u;  stage 2: u = u + x - z. */
+int hb_svt_blocks(void* x, int64_t d0, int64_t d1, int64_t S0, int64_t S1, int64_t S2, int64_t b0, int64_t b1,
+                  int64_t b2, const int32_t* corners, int64_t nblocks, double thresh, int soft, void* stream);
+int hb_admm_vectors(int64_t n, int stage, const void* x, void* z, void* u, const void* b0, void* b, float rho,
+                    void* stream);
+
 /* ---- measurement hooks (no counterpart in the reference; used by benchmarks) ----
  * Kernel kinds for the profile counters. */
 #define HB_KERNEL_EXPAND_FWD_X 0   /* pass A */

@@ -26,6 +26,8 @@ LibTorch).  File references below are paths inside the reference project:
   forward / adjoint around them (``lib/mri/sense.ixx:426-497``), as direct NUDFTs.
 * ``lib/mri/precond.cpp:65-117`` the circulant preconditioner (the Fourier-domain diagonal of
   the SENSE normal operator, inverted) and its apply.
+* ``lib/op/svt.cpp:11-490`` block singular-value thresholding (locally low rank) and the
+  scaled ADMM around CG (``lib/op/opalgs.cpp:103-111``, ``lib/mri/batch_sense.ixx:302-431``).
 * ``lib/fft/nufft.cpp:410-767`` / ``:785-920`` explicit NUFFT normal op on the N grid
   (type-2 then type-1, each /sqrt(prod(N))), evaluated as a dense direct NUDFT.
   ``Toeplitz = explicit / 2^3`` in 3D because of the two different grid scalings.
@@ -200,6 +202,47 @@ def precond_apply(P, x):
     """``CirculantPreconditionerOp::apply`` (``precond.cpp:30-52``) in FFT order:
     IFFT(P * FFT(x))."""
     return np.fft.ifftn(P * np.fft.fftn(np.asarray(x, np.complex128)))
+
+
+def svt_blocks(x, corners, block_shape, thresh, soft=True):
+    """Block singular-value thresholding (``lib/op/svt.cpp``): for each corner in order,
+    extract the block of x [d0, d1, S0, S1, S2] as the matrix [d1*b0*b1*b2, d0]
+    (``extract_block``, ``:11-58``), threshold its singular values (``svt_soft`` /
+    ``svt_hard``, ``:60-168``: soft s -> max(s - thresh, 0), hard keeps round(thresh)) and
+    insert it back (``insert_block``, ``:170-240``).  float64."""
+    y = np.array(x, np.complex128)
+    d0, d1 = y.shape[:2]
+    b0, b1, b2 = block_shape
+    for c0, c1, c2 in corners:
+        sl = (slice(None), slice(None), slice(c0, c0 + b0), slice(c1, c1 + b1), slice(c2, c2 + b2))
+        M = y[sl].reshape(d0, -1).T
+        U, S, Vh = np.linalg.svd(M, full_matrices=False)
+        if soft:
+            S = np.maximum(S - thresh, 0.0)
+        else:
+            S[int(thresh + 0.5):] = 0.0
+        y[sl] = ((U * S) @ Vh).T.reshape(d0, d1, b0, b1, b2)
+    return y
+
+
+def admm_llr(A_of_system, b0, x0, rho, svt, admm_iters, cg_iters):
+    """Scaled ADMM for min ||S x - y||^2 + R(z) s.t. x = z (``lib/op/opalgs.cpp:103-111``,
+    ``lib/mri/batch_sense.ixx:302-431``): x-update by CG on (A + rho/2 I) x = b0 + rho/2 (z - u)
+    per system (A_of_system(s) is system s's normal operator), z = prox(x + u), u += x - z.
+    x0, b0: [d0, d1, *image]; svt(v) returns the proximal step of v."""
+    x = np.array(x0, np.complex128)
+    z = x.copy()
+    u = np.zeros_like(x)
+    d0, d1 = x.shape[:2]
+    for _ in range(admm_iters):
+        b = b0 + 0.5 * rho * (z - u)
+        for f in range(d0):
+            for e in range(d1):
+                A = regularized(A_of_system(f, e), 0.5 * rho)
+                x[f, e], _ = conjugate_gradient(A, b[f, e], x0=x[f, e], iters=cg_iters)
+        z = svt(x + u)
+        u = u + x - z
+    return x, z
 
 
 def vdot(a, b):
