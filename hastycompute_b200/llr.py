@@ -24,24 +24,28 @@ from . import capi
 from .toeplitz import _check_c64, _ptr, _stream_ptr
 
 
-def _overlaps(corners, c, shape):
-    if len(corners) == 0:
-        return False
-    a = np.asarray(corners)
-    return bool(np.any(np.all(np.abs(a - np.asarray(c)) < np.asarray(shape), axis=1)))
-
-
-def waves_of(corners, block_shape):
+def waves_of(corners, block_shape, space_shape=None):
     """Greedy partition of block corners into lists of non-overlapping blocks, keeping the
-    input order within and across waves as far as possible."""
-    waves = []
-    for c in corners:
-        for w in waves:
-            if not _overlaps(w, c, block_shape):
-                w.append(tuple(int(v) for v in c))
+    input order within and across waves; one voxel-occupancy grid per wave."""
+    cs = [tuple(int(v) for v in c) for c in corners]
+    if not cs:
+        return []
+    b = tuple(int(v) for v in block_shape)
+    if space_shape is None:
+        space_shape = tuple(max(c[d] for c in cs) + b[d] for d in range(3))
+    waves, occ = [], []
+    for c in cs:
+        sl = tuple(slice(c[d], c[d] + b[d]) for d in range(3))
+        for w, o in zip(waves, occ):
+            if not o[sl].any():
+                w.append(c)
+                o[sl] = True
                 break
         else:
-            waves.append([tuple(int(v) for v in c)])
+            o = np.zeros(space_shape, bool)
+            o[sl] = True
+            waves.append([c])
+            occ.append(o)
     return waves
 
 
@@ -92,7 +96,7 @@ class Random3DBlocksSVT(_BlocksSVT):
     def apply(self, x):
         bounds = [s - b for s, b in zip(self.input_shape[2:], self.block_shape)]
         corners = [tuple(int(self.rng.integers(0, bd + 1)) for bd in bounds) for _ in range(self.nblocks)]
-        return self._run(x, waves_of(corners, self.block_shape))
+        return self._run(x, waves_of(corners, self.block_shape, self.input_shape[2:]))
 
 
 class Normal3DBlocksSVT(_BlocksSVT):
@@ -132,9 +136,13 @@ class Normal3DBlocksSVT(_BlocksSVT):
 
     def apply(self, x):
         waves = []
+        disjoint = all(st >= b for st, b in zip(self.block_strides, self.block_shape))
         for cs in self.corners():  # iterations in order; overlapping blocks of one iteration split into waves
-            waves.extend(waves_of(cs, self.block_shape))
-        return self._run(x, waves)
+            if disjoint:
+                waves.append(cs)
+            else:
+                waves.extend(waves_of(cs, self.block_shape, self.input_shape[2:]))
+        return self._run(x, [w for w in waves if w])
 
 
 def admm_vectors(stage, x, z, u, b0=None, b=None, rho=1.0):
