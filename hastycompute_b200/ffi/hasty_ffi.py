@@ -5,7 +5,7 @@ _PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def get_ffi_libfile():
-    """The TorchScript library with the HastyToeplitz classes."""
+    """The TorchScript library with the HastyToeplitz, HastyNufft and HastySVT classes."""
     return os.path.join(_PKG, "libhasty_torch.so")
 
 

@@ -109,3 +109,36 @@ def test_errors_are_runtime_errors(ffi, cuda):
     sm = torch.ones((2, 8, 8, 8), dtype=torch.complex64, device=cuda)
     with pytest.raises(RuntimeError, match="coil index"):
         op.apply(x, torch.empty_like(x), sm, [0, 5])
+
+
+def test_nufft_and_svt_torchscript_classes(cuda):
+    """torch.classes.HastyNufft / HastySVT through the reference-named wrappers."""
+    from hastycompute_b200.ffi import hasty_nufft, hasty_svt
+
+    shape, K = (8, 16, 16), 1200
+    rng = np.random.default_rng(9)
+    coords_np = rng.uniform(-np.pi, np.pi, (3, K)).astype(np.float32)
+    coords = torch.from_numpy(coords_np).to(cuda)
+    c = rng.standard_normal((2, K)) + 1j * rng.standard_normal((2, K))
+    op = hasty_nufft.Nufft(coords, [2, *shape], hasty_nufft.NufftOptions(1, True, 1e-6))
+    out = torch.empty((2, *shape), dtype=torch.complex64, device=cuda)
+    op.apply(torch.from_numpy(c.astype(np.complex64)).to(cuda), out)
+    assert O.rel_l2(_np(out), O.nudft_type1(coords_np, c, shape, +1)) < 1e-5
+    nn = hasty_nufft.NufftNormal(coords, [1, *shape], hasty_nufft.NufftOptions(2, False, 1e-6),
+                                 hasty_nufft.NufftOptions(1, True, 1e-6))
+    x = synth.gaussian_image(shape, seed=10)
+    y = torch.empty((1, *shape), dtype=torch.complex64, device=cuda)
+    st = torch.empty((1, K), dtype=torch.complex64, device=cuda)
+    nn.apply(torch.from_numpy(x[None].astype(np.complex64)).to(cuda), y, st)
+    assert O.rel_l2(_np(y[0]) / np.prod(shape), O.explicit_normal(x, coords_np)) < 1e-5
+    with pytest.raises(RuntimeError, match="nmodes"):
+        op.apply(torch.from_numpy(c.astype(np.complex64)).to(cuda), torch.empty((3, *shape), dtype=torch.complex64,
+                                                                              device=cuda))
+    # SVT on a CPU tensor (moved to the GPU and back, as the reference moves its blocks)
+    v = (rng.standard_normal((6, 2, 16, 16, 16)) + 1j * rng.standard_normal((6, 2, 16, 16, 16))).astype(np.complex64)
+    vt = torch.from_numpy(v.copy())
+    hasty_svt.Normal3DBlocksSVT().apply(vt, [8, 8, 8], [7, 7, 7], 1, 1.5, True)
+    ref = O.svt_blocks(v, [(0, 0, 0), (0, 0, 8), (0, 8, 0), (0, 8, 8), (8, 0, 0), (8, 0, 8), (8, 8, 0), (8, 8, 8)],
+                       (7, 7, 7), 1.5, True)
+    assert O.rel_l2(vt.numpy().astype(np.complex128), ref) < 1e-5
+    hasty_svt.Random3DBlocksSVT().apply(vt, 10, [4, 4, 4], 2, False)  # runs; the corners are internal
