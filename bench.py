@@ -191,9 +191,10 @@ MIX_COILS = [8, 12, 16, 32]
 def make_job_mix(a, dev, njobs, plans):
     """Seeded job mix: image size from MIX_SHAPES, coils from MIX_COILS, 1..max_frames
     frames (one system per frame), a golden-angle kooshball of 1000-4000 spokes x 256.
-    The job's diagonal is built in FP64 from its trajectory and shared by its frames
+    The job's diagonal is built from its trajectory (``--diag``; the NUFFT route falls back
+    to the exact build for 96^3 and 160^2 images) and shared by its frames
     (solve timing does not depend on the diagonal's values); b is a seeded random image."""
-    from hastycompute_b200 import synth
+    from hastycompute_b200 import capi, synth
     from hastycompute_b200.toeplitz import ToeplitzPlan
 
     rng = np.random.default_rng(a.seed)
@@ -208,7 +209,12 @@ def make_job_mix(a, dev, njobs, plans):
             plans[shape] = ToeplitzPlan(shape, dev)
         plan = plans[shape]
         coords = torch.from_numpy(synth.kooshball(spokes, a.samples, frame=j % 7, nframes=7))
-        packed = plan.build_diagonal(coords, method=a.diag).unsqueeze(0)
+        try:
+            packed = plan.build_diagonal(coords, method=a.diag).unsqueeze(0)
+        except capi.HastyError as e:  # the NUFFT route needs 4N among its grid lengths (not 96, 160)
+            if e.code != capi.HB_ERR_UNSUPPORTED:
+                raise
+            packed = plan.build_diagonal(coords, method="exact").unsqueeze(0)
         sm = synth.coil_maps_torch(ncoil, shape, seed=1000 + j, device=dev)
         b = torch.randn((nframes,) + shape, dtype=torch.complex64, device=dev, generator=g)
         jobs.append({"shape": shape, "smaps": sm, "packed": packed, "b": b, "frames": nframes, "coils": ncoil,

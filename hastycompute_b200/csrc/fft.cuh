@@ -292,6 +292,7 @@ constexpr int team_buf_stride() {
 template <int L, int DIR, bool HALF_IN>
 __device__ __forceinline__ void team_fft_din_to_dout(float2* v, int t, float2* buf, const float2* tw) {
   constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+  static_assert(E % S == 0, "a lane runs E/S S-point DFTs after the exchange: S must divide E");
   if constexpr (HALF_IN) DftHalfIn<E, DIR>::run(v);
   else Dft<E, DIR>::run(v);
 #pragma unroll

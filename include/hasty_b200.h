@@ -214,7 +214,7 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
  *   type 2:  c[j] = sum_k f[k] exp(isign * i * k . x_j)      (reference: isign = -1)
  * Method: exponential-of-semicircle gridding kernel with upsampling 2 (the published
  * method of finufft); kernel width w = ceil(log10(1/tol)) + 1 fine-grid cells.
- * 2*N_a must be one of 8, 16, 32, 64, 128, 256, 96, 160, 192, 320 and >= 2w.
+ * 2*N_a must be one of 8, 16, 32, 64, 128, 256, 512, 96, 160, 192, 320 and >= 2w.
  * Type 1 accumulates with atomics, so its last bits vary from run to run.
  *
  * hb_nufft_create copies coords, sorts the samples by fine-grid bin and allocates the
@@ -251,7 +251,8 @@ int hb_sense_normal_nufft(const hb_nufft* plan, const void* x, const void* smaps
  * type-1 NUFFT of unit weights onto the 2x grid's modes, shifted to circulant layout and
  * scaled by 1/prod(2N), then FFT'd.  Same outputs as hb_diag_build (packed and/or the
  * complex T [2nz][2ny][2nx]) to the NUFFT tolerance instead of FP64-exact, in
- * milliseconds instead of seconds.  Allocates its NUFFT plan (a (4nz)(4ny)(4nx)
+ * milliseconds instead of seconds.  Needs 4*N per axis among the NUFFT's fine-grid lengths
+ * (image axes of 8..128; HB_ERR_UNSUPPORTED for 96 and 160, use hb_diag_build there).  Allocates its NUFFT plan (a (4nz)(4ny)(4nx)
  * complex64 fine grid) for the duration of the call and synchronises `stream`. */
 int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsamples, double tol, float* packed,
                         void* T_complex, void* stream);

@@ -169,3 +169,13 @@ def test_diagonal_through_the_nufft_matches_the_exact_build(cuda, shape):
     assert O.rel_l2(_np(Tn), T) < 1e-5
     with pytest.raises(RuntimeError, match="method"):
         plan.build_diagonal(coords, method="fast")
+
+
+@pytest.mark.parametrize("shape", [(96, 96, 8), (160, 160, 8)])
+def test_diagonal_through_the_nufft_rejects_unsupported_grids(cuda, shape):
+    """4*96 and 4*160 are not fine-grid lengths of the NUFFT: the build says so."""
+    coords = torch.from_numpy(_coords(500, 23)).to(cuda)
+    plan = ToeplitzPlan(shape, cuda)
+    with pytest.raises(capi.HastyError) as e:
+        plan.build_diagonal(coords, method="nufft")
+    assert e.value.code == capi.HB_ERR_UNSUPPORTED
