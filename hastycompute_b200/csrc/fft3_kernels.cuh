@@ -78,10 +78,14 @@ __global__ void __launch_bounds__(LineCfg<L>::THREADS_S) fft_lines_strided_kerne
   float2* base = data + (long long)blockIdx.y * oy_stride + (long long)blockIdx.z * oz_stride + x0;
   const int nc = (ncols - x0) < XT ? (ncols - x0) : XT;
   for (int i = threadIdx.x; i < L; i += C::THREADS_S) tws[i] = tw[i];
+  // the tile arrives by asynchronous copies, all in flight at once
   for (int i = threadIdx.x; i < L * XT; i += C::THREADS_S) {
     const int r = i / XT, c = i % XT;
-    tile[r * LD + c] = c < nc ? base[(long long)r * row_stride + c] : make_float2(0.f, 0.f);
+    if (c < nc) cp_async8(&tile[r * LD + c], base + (long long)r * row_stride + c);
+    else tile[r * LD + c] = make_float2(0.f, 0.f);
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   const int team = threadIdx.x / S, t = threadIdx.x % S;  // team = tile column
   {

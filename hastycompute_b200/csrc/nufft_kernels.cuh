@@ -14,7 +14,7 @@
 // FFT with sign isign, divide by phi_hat(k) and crop; type 2 = the transpose.
 //
 // Samples are bucketed by fine-grid bin once per plan (counting sort), so that spreading
-// (float2 atomics into global memory) and interpolation (gathers) walk the grid with
+// (vector reductions into global memory) and interpolation (gathers) walk the grid with
 // locality.  The atomics make type 1 bitwise non-deterministic, as the reference's
 // cufinufft is.
 #pragma once
@@ -59,6 +59,11 @@ __device__ __forceinline__ int nufft_axis_weights(float u, float beta, float* wt
 }
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// *p += v as one vector reduction (no value returned, so the issuing warp does not wait)
+__device__ __forceinline__ void red_add(float2* p, float2 v) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v.x), "f"(v.y) : "memory");
+}
 
 // ---- binning (once per plan) ----
 __global__ void nufft_bin_count_kernel(NufftGeom g, const float* coords, int* sample_bin, int* bin_count) {
@@ -129,7 +134,7 @@ __global__ void __launch_bounds__(256) nufft_spread_kernel(NufftGeom g, const fl
       const float2 cab = cscale(ca, w1[b]);
       float2* Gab = Ga + (long long)wrap(i1 + b, g.n[1]) * g.n[2];
 #pragma unroll
-      for (int m = 0; m < W; ++m) atomicAdd(Gab + x2[m], cscale(cab, w2[m]));
+      for (int m = 0; m < W; ++m) red_add(Gab + x2[m], cscale(cab, w2[m]));
     }
   }
 }
