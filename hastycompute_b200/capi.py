@@ -79,10 +79,11 @@ SIGNATURES = {
     "hb_nufft_width": (c_int, [c_void_p]),
     "hb_nufft_type1": (c_int, [c_void_p, c_void_p, c_void_p, c_i64, c_int, c_void_p]),
     "hb_nufft_type2": (c_int, [c_void_p, c_void_p, c_void_p, c_i64, c_int, c_void_p]),
-    "hb_sense_adjoint_nufft": (c_int, [c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, c_int, c_void_p]),
+    "hb_sense_adjoint_nufft": (c_int, [c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, c_void_p, c_int,
+                                       c_void_p]),
     "hb_sense_normal_nufft": (c_int, [c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, c_void_p, c_void_p,
                                       c_int, c_void_p]),
-    "hb_diag_build_nufft": (c_int, [c_void_p, c_void_p, c_i64, c_double, c_void_p, c_void_p, c_void_p]),
+    "hb_diag_build_nufft": (c_int, [c_void_p, c_void_p, c_i64, c_double, c_void_p, c_void_p, c_void_p, c_void_p]),
     "hb_sense_forward_nufft": (c_int, [c_void_p, c_void_p, c_void_p, P_i64, c_i64, c_void_p, c_void_p]),
     "hb_precond_build": (c_int, [c_void_p, c_void_p, c_i64, c_double, c_void_p, P_i64, c_i64, c_float, c_void_p,
                                  c_void_p]),

@@ -172,8 +172,8 @@ void free_plan(hb_nufft* p) {
 
 namespace hb {
 
-int nufft_psf_circulant(const int* M, const float* coords, int64_t nsamples, double tol, int device, float2* out,
-                        cudaStream_t st) {
+int nufft_psf_circulant(const int* M, const float* coords, int64_t nsamples, double tol, const float* weights,
+                        int device, float2* out, cudaStream_t st) {
   const long long vol = (long long)M[0] * M[1] * M[2];
   hb_nufft* np = nullptr;
   // type 1 over the grid's modes: sum_j exp(+i c_j . d), d in [-M/2, M/2)
@@ -184,7 +184,8 @@ int nufft_psf_circulant(const int* M, const float* coords, int64_t nsamples, dou
   if (e == cudaSuccess) {
     {
       LaunchScope ls(HB_KERNEL_DIAG, st);
-      fill_c64_kernel<<<(unsigned)((nsamples + 255) / 256), 256, 0, st>>>(ones, nsamples, make_float2(1.f, 0.f));
+      fill_c64_kernel<<<(unsigned)((nsamples + 255) / 256), 256, 0, st>>>(ones, nsamples, make_float2(1.f, 0.f),
+                                                                          weights);
     }
     rc = type1_batch(np, ones, nsamples, np->modes, vol, 1, +1, st);
     if (rc == HB_OK) {
@@ -335,7 +336,7 @@ int hb_nufft_type2(const hb_nufft* plan, const void* f, void* c, int64_t ntransf
 }
 
 int hb_sense_adjoint_nufft(const hb_nufft* plan, const void* kdata, const void* smaps, const int64_t* coils,
-                           int64_t ncoil, void* out, int accumulate, void* stream) {
+                           int64_t ncoil, const float* weights, void* out, int accumulate, void* stream) {
   if (!plan || !kdata || !smaps || !out || ncoil < 0 || (ncoil > 0 && !coils))
     return fail(HB_ERR_INVALID, "hb_sense_adjoint_nufft: null argument or negative ncoil");
   for (int64_t b = 0; b < ncoil; ++b)
@@ -343,11 +344,22 @@ int hb_sense_adjoint_nufft(const hb_nufft* plan, const void* kdata, const void* 
   DeviceGuard dg(plan->device);
   cudaStream_t st = (cudaStream_t)stream;
   const long long K = plan->g.K, nm = nmodes(plan);
-  const unsigned vb = (unsigned)((nm + 255) / 256);
+  const unsigned vb = (unsigned)((nm + 255) / 256), kb = (unsigned)((K + 255) / 256);
   if (ncoil == 0 && !accumulate) HB_CUDA(cudaMemsetAsync(out, 0, nm * sizeof(float2), st));
   for (int64_t b0 = 0; b0 < ncoil; b0 += plan->maxbatch) {
     const int nb = (int)((ncoil - b0) < plan->maxbatch ? (ncoil - b0) : plan->maxbatch);
-    if (int r = type1_batch(plan, (const float2*)kdata + b0 * K, K, plan->modes, nm, nb, +1, st)) return r;
+    const float2* src = (const float2*)kdata + b0 * K;
+    if (weights) {  // w * kdata rows into the plan's k-space temporaries
+      KdataPtrs ys{};
+      for (int b = 0; b < nb; ++b) ys.y[b] = src + b * K;
+      {
+        LaunchScope ls(HB_KERNEL_NUFFT, st);
+        sense_kspace_weight_kernel<<<kb, 256, 0, st>>>(plan->kbuf, nb, K, ys, weights);
+      }
+      HB_CHECK_LAUNCH();
+      src = plan->kbuf;
+    }
+    if (int r = type1_batch(plan, src, K, plan->modes, nm, nb, +1, st)) return r;
     CoilMaps maps{};
     for (int b = 0; b < nb; ++b) maps.s[b] = (const float2*)smaps + coils[b0 + b] * nm;
     {
@@ -425,8 +437,8 @@ int hb_sense_normal_nufft(const hb_nufft* plan, const void* x, const void* smaps
   return HB_OK;
 }
 
-int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsamples, double tol, float* packed,
-                        void* T_complex, void* stream) {
+int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsamples, double tol, const float* weights,
+                        float* packed, void* T_complex, void* stream) {
   if (!plan || !coords || nsamples < 1) return fail(HB_ERR_INVALID, "hb_diag_build_nufft: null plan or no samples");
   if (!packed && !T_complex) return fail(HB_ERR_INVALID, "hb_diag_build_nufft: no output requested");
   int N[3], dev = 0;
@@ -452,7 +464,7 @@ int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsampl
       break;
     }
     // PSF in circulant layout on the 2x grid, then T = FFT(PSF)
-    if ((rc = nufft_psf_circulant(M, coords, nsamples, tol, dev, T, st)) != HB_OK) break;
+    if ((rc = nufft_psf_circulant(M, coords, nsamples, tol, weights, dev, T, st)) != HB_OK) break;
     if ((e = fft3_grid<-1>(M[0], M[1], M[2], tw, T, 1, st)) != cudaSuccess) { cuda_fail(e, "fft"); break; }
     if (packed && (rc = hb_diag_pack(plan, T, packed, stream)) != HB_OK) break;
     if (T_complex &&

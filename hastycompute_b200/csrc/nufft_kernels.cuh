@@ -212,9 +212,10 @@ __global__ void nufft_precorrect_kernel(NufftGeom g, const float2* f, long long 
 }
 
 // ---- Toeplitz diagonal through the NUFFT ----
-__global__ void fill_c64_kernel(float2* a, long long n, float2 v) {
+// a[i] = v, times w[i] when w is given
+__global__ void fill_c64_kernel(float2* a, long long n, float2 v, const float* w) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) a[i] = v;
+  if (i < n) a[i] = w ? cscale(v, w[i]) : v;
 }
 
 // Circulant (ifftshift) layout of a centred [M0][M1][M2] array, scaled:
@@ -258,6 +259,14 @@ __global__ void sense_kspace_mid_kernel(float2* k, int nb, long long K, KdataPtr
     if (y.y[b]) v = csub(v, y.y[b][j]);
     k[b * K + j] = cscale(v, wj);
   }
+}
+
+// k[b][j] = y_b[j] * w[j]  (weighted copy of k-space rows)
+__global__ void sense_kspace_weight_kernel(float2* k, int nb, long long K, KdataPtrs y, const float* w) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= K) return;
+  const float wj = w[j];
+  for (int b = 0; b < nb; ++b) k[b * K + j] = cscale(y.y[b][j], wj);
 }
 
 // f[b] = S_b * x

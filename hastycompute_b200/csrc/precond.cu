@@ -116,7 +116,7 @@ int hb_precond_build(const hb_plan* plan, const float* coords, int64_t nsamples,
   do {
     cudaError_t e;
     if ((e = cudaMalloc(&psf, vol * sizeof(float2))) != cudaSuccess) { cuda_fail(e, "alloc"); break; }
-    if ((rc = nufft_psf_circulant(M, coords, nsamples, tol, dev, psf, st)) != HB_OK) break;
+    if ((rc = nufft_psf_circulant(M, coords, nsamples, tol, nullptr, dev, psf, st)) != HB_OK) break;
     if ((e = cudaMalloc(&G, (size_t)nb * vol * sizeof(float2))) != cudaSuccess) { cuda_fail(e, "alloc"); break; }
     if ((e = cudaMalloc(&Q, vol * sizeof(float))) != cudaSuccess) { cuda_fail(e, "alloc"); break; }
     const std::vector<float2> tables = fftl::team_tables(M);

@@ -21,11 +21,12 @@ namespace hb {
 void plan_geometry(const ::hb_plan* plan, int* N, int* device);
 const float2* plan_image_tables(const ::hb_plan* plan);
 
-// psf(d) = prod(M)^-1 * sum_j exp(+i c_j . d) on an M0 x M1 x M2 grid in circulant layout
+// psf(d) = prod(M)^-1 * sum_j w_j exp(+i c_j . d) (w_j = 1 when weights is null) on an
+// M0 x M1 x M2 grid in circulant layout
 // (offset d = n for n < M/2, n - M otherwise), through a type-1 NUFFT at tolerance tol;
 // out: [M0][M1][M2] complex64.  Synchronises st.
-int nufft_psf_circulant(const int* M, const float* coords, int64_t nsamples, double tol, int device, float2* out,
-                        cudaStream_t st);
+int nufft_psf_circulant(const int* M, const float* coords, int64_t nsamples, double tol, const float* weights,
+                        int device, float2* out, cudaStream_t st);
 
 // Message of the last failure on this thread (hb_last_error).
 inline thread_local std::string g_err;

@@ -106,8 +106,9 @@ class NufftPlan:
                                            _stream_ptr(self.device)))
         return c
 
-    def sense_adjoint(self, kdata, smaps, coils=None, out=None, accumulate=False):
-        """out (+)= sum_b conj(smaps[coils[b]]) * type1(kdata[b])."""
+    def sense_adjoint(self, kdata, smaps, coils=None, out=None, accumulate=False, weights=None):
+        """out (+)= sum_b conj(smaps[coils[b]]) * type1(w * kdata[b]) (w: optional float32
+        [nfreq] sample weights)."""
         coils = list(range(smaps.shape[0])) if coils is None else [int(c) for c in coils]
         kdata = kdata.reshape(len(coils), self.nfreq)
         _check_c64(kdata, "kdata", self.device)
@@ -116,9 +117,14 @@ class NufftPlan:
             out = torch.empty(self.shape, dtype=torch.complex64, device=self.device)
             accumulate = False
         _check_c64(out, "out", self.device, self.shape)
+        if weights is not None:
+            weights = weights.reshape(-1)
+            if weights.dtype != torch.float32 or weights.numel() != self.nfreq or weights.device != self.device \
+                    or not weights.is_contiguous():
+                raise RuntimeError("weights must be a contiguous float32 [nfreq] tensor on the device")
         arr = (ctypes.c_int64 * max(1, len(coils)))(*coils)
-        capi.check(self.lib.hb_sense_adjoint_nufft(self._h, _ptr(kdata), _ptr(smaps), arr, len(coils), _ptr(out),
-                                                   1 if accumulate else 0, _stream_ptr(self.device)))
+        capi.check(self.lib.hb_sense_adjoint_nufft(self._h, _ptr(kdata), _ptr(smaps), arr, len(coils), _ptr(weights),
+                                                   _ptr(out), 1 if accumulate else 0, _stream_ptr(self.device)))
         return out
 
     def sense_normal(self, x, smaps, coils=None, kdata=None, weights=None, out=None, accumulate=False):

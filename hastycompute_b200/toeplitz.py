@@ -111,12 +111,13 @@ class ToeplitzPlan:
         return chosen.value, ms.value
 
     # ---------------------------------------------------------------- diagonal ----
-    def build_diagonal(self, coords, want_complex=False, method="exact", tol=1e-6):
+    def build_diagonal(self, coords, want_complex=False, method="exact", tol=1e-6, weights=None):
         """Construction of T from a trajectory coords [3, K] float32 (radians).
 
         method "exact": FP64 direct sum (``hb_diag_build``); "nufft": the reference's own
         construction through a type-1 NUFFT at tolerance ``tol`` (``hb_diag_build_nufft``,
-        ``nufft.cpp:932-971``), much faster for long trajectories.
+        ``nufft.cpp:932-971``), much faster for long trajectories, optionally with sample
+        ``weights`` (density compensation).
         Returns the packed diagonal (float32) and, if requested, the reference-layout
         complex64 T [2nz, 2ny, 2nx]."""
         if coords.dtype != torch.float32 or coords.dim() != 2 or coords.shape[0] != 3:
@@ -125,9 +126,15 @@ class ToeplitzPlan:
         K = coords.shape[1]
         packed = torch.empty(self.packed_numel(), dtype=torch.float32, device=self.device)
         T = torch.empty(self.grid, dtype=torch.complex64, device=self.device) if want_complex else None
+        if weights is not None:
+            if method != "nufft":
+                raise RuntimeError("sample weights need method='nufft'")
+            weights = weights.to(self.device, torch.float32).reshape(-1).contiguous()
+            if weights.numel() != K:
+                raise RuntimeError("weights must hold one value per sample")
         if method == "nufft":
-            capi.check(self.lib.hb_diag_build_nufft(self._h, _ptr(coords), K, float(tol), _ptr(packed), _ptr(T),
-                                                    _stream_ptr(self.device)))
+            capi.check(self.lib.hb_diag_build_nufft(self._h, _ptr(coords), K, float(tol), _ptr(weights), _ptr(packed),
+                                                    _ptr(T), _stream_ptr(self.device)))
         elif method == "exact":
             nb = self.lib.hb_diag_build_workspace_bytes(self._h, K)
             ws = torch.empty(int(nb), dtype=torch.uint8, device=self.device)

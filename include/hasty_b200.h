@@ -230,12 +230,12 @@ int hb_nufft_width(const hb_nufft* plan);
 int hb_nufft_type1(const hb_nufft* plan, const void* c, void* f, int64_t ntransf, int isign, void* stream);
 int hb_nufft_type2(const hb_nufft* plan, const void* f, void* c, int64_t ntransf, int isign, void* stream);
 
-/* SENSE adjoint: out (+)= sum_b conj(S[coils[b]]) * type1(kdata[b]) (isign +1), kdata
- * [ncoil][nsamples], smaps [*][nz][ny][nx], coils a HOST array of ncoil map indices;
- * accumulate = 0 overwrites out.  The CG right-hand side of the reference's SENSE
- * reconstructions. */
+/* SENSE adjoint: out (+)= sum_b conj(S[coils[b]]) * type1(w * kdata[b]) (isign +1), kdata
+ * [ncoil][nsamples], smaps [*][nz][ny][nx], coils a HOST array of ncoil map indices,
+ * weights float32 [nsamples] (nullable: w = 1); accumulate = 0 overwrites out.  The CG
+ * right-hand side of the reference's SENSE reconstructions (reconstruct_util.py:69-87). */
 int hb_sense_adjoint_nufft(const hb_nufft* plan, const void* kdata, const void* smaps, const int64_t* coils,
-                           int64_t ncoil, void* out, int accumulate, void* stream);
+                           int64_t ncoil, const float* weights, void* out, int accumulate, void* stream);
 /* SENSE normal operator through the NUFFT with the reference's k-space manipulators
  * (BatchedSenseNormal standard_kdata / standard_weighted / standard_weighted_kdata
  * manipulators, lib/mri/batch_sense.cpp:452-486; the coil loop of sense.ixx:426-497):
@@ -248,14 +248,16 @@ int hb_sense_normal_nufft(const hb_nufft* plan, const void* x, const void* smaps
 
 /* Toeplitz diagonal through the NUFFT, the reference's own construction
  * (build_diagonal_base, lib/fft/nufft.cpp:932-971, at tolerance `tol`): the PSF is a
- * type-1 NUFFT of unit weights onto the 2x grid's modes, shifted to circulant layout and
+ * type-1 NUFFT of the sample weights (nullable float32 [nsamples], 1 when NULL; the
+ * density-compensated kernel of reconstruct_util.py:59-66) onto the 2x grid's modes,
+ * shifted to circulant layout and
  * scaled by 1/prod(2N), then FFT'd.  Same outputs as hb_diag_build (packed and/or the
  * complex T [2nz][2ny][2nx]) to the NUFFT tolerance instead of FP64-exact, in
  * milliseconds instead of seconds.  Needs 4*N per axis among the NUFFT's fine-grid lengths
  * (image axes of 8..128; HB_ERR_UNSUPPORTED for 96 and 160, use hb_diag_build there).  Allocates its NUFFT plan (a (4nz)(4ny)(4nx)
  * complex64 fine grid) for the duration of the call and synchronises `stream`. */
-int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsamples, double tol, float* packed,
-                        void* T_complex, void* stream);
+int hb_diag_build_nufft(const hb_plan* plan, const float* coords, int64_t nsamples, double tol, const float* weights,
+                        float* packed, void* T_complex, void* stream);
 
 /* SENSE forward: kdata[b] = type2(S[coils[b]] * x) (isign -1). */
 int hb_sense_forward_nufft(const hb_nufft* plan, const void* x, const void* smaps, const int64_t* coils,
