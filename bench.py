@@ -436,14 +436,12 @@ def main():
         xh = torch.zeros((nsys,) + shape, dtype=torch.complex64).pin_memory()
         bh = b.cpu().pin_memory()
         outh = torch.empty_like(xh).pin_memory()
-        xd = torch.empty_like(x)
-        bd = torch.empty_like(b)
 
         def e2e_step():
-            xd.copy_(xh, non_blocking=True)
-            bd.copy_(bh, non_blocking=True)
-            plan.cg(xd, bd, sm, packed, iters=a.iters, lam=a.lam, diag_index=diag_index)
-            outh.copy_(xd, non_blocking=True)
+            # initial guess and right-hand side from pinned host memory, solution back to it;
+            # cg_host overlaps the copies of one group of systems with the solve of another
+            plan.cg_host(xh, bh, sm, packed, iters=a.iters, lam=a.lam, diag_index=diag_index, chunks=4,
+                         out_host=outh)
 
         e2e_step()
         torch.cuda.synchronize()

@@ -294,6 +294,62 @@ class ToeplitzPlan:
         capi.check(self.lib.hb_precond_apply(self._h, _ptr(precond), _ptr(x), _ptr(out), _stream_ptr(self.device)))
         return out
 
+    def cg_host(self, x_host, b_host, smaps, packed, iters=30, tol=0.0, lam=0.0, coils=None, diag_index=None,
+                chunks=4, raise_not_pd=True, out_host=None):
+        """CG for systems whose initial guess and right-hand side live in (pinned) host memory;
+        the solution is written into ``out_host`` (default: back into ``x_host``).  The systems are solved in ``chunks``
+        consecutive groups: all host-to-device copies are issued first on a copy stream, each
+        group's solve waits only for its own data, and each group's solution is copied back
+        while the next group is solved, so the copy engines work beside the SMs (the
+        reference copies every inner batch to and from the host synchronously,
+        ``batch_sense.cpp:349-450``).  Returns (status, iters_done) as lists."""
+        x4 = x_host.reshape((-1,) + self.shape)
+        b4 = b_host.reshape((-1,) + self.shape)
+        o4 = x4 if out_host is None else out_host.reshape((-1,) + self.shape)
+        nsys = x4.shape[0]
+        if o4.shape[0] != nsys:
+            raise RuntimeError("out_host must hold every system")
+        if b4.shape[0] != nsys or x4.dtype != torch.complex64 or b4.dtype != torch.complex64:
+            raise RuntimeError("x_host and b_host must be complex64 with the same number of systems")
+        if diag_index is None:
+            diag_index = [0] * nsys
+        main = torch.cuda.current_stream(self.device)
+        if getattr(self, "_copy_stream", None) is None:
+            self._copy_stream = torch.cuda.Stream(self.device)
+        cs = self._copy_stream
+        xd = torch.empty(x4.shape, dtype=torch.complex64, device=self.device)
+        bd = torch.empty(b4.shape, dtype=torch.complex64, device=self.device)
+        bounds = [round(k * nsys / max(1, chunks)) for k in range(max(1, chunks) + 1)]
+        ready = []
+        cs.wait_stream(main)  # the device buffers may be reused memory
+        with torch.cuda.stream(cs):
+            for k in range(len(bounds) - 1):
+                sl = slice(bounds[k], bounds[k + 1])
+                xd[sl].copy_(x4[sl], non_blocking=True)
+                bd[sl].copy_(b4[sl], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(cs)
+                ready.append(ev)
+        status, done = [], []
+        try:
+            for k in range(len(bounds) - 1):
+                lo, hi = bounds[k], bounds[k + 1]
+                if hi <= lo:
+                    continue
+                main.wait_event(ready[k])
+                st, it = self.cg(xd[lo:hi], bd[lo:hi], smaps, packed, iters=iters, tol=tol, lam=lam, coils=coils,
+                                 diag_index=list(diag_index[lo:hi]), raise_not_pd=raise_not_pd)
+                status += st
+                done += it
+                cs.wait_stream(main)
+                with torch.cuda.stream(cs):
+                    o4[lo:hi].copy_(xd[lo:hi], non_blocking=True)
+        finally:
+            main.wait_stream(cs)
+            xd.record_stream(cs)
+            bd.record_stream(cs)
+        return status, done
+
     # ------------------------------------------------------- heterogeneous batch ----
     def _systems(self, systems, cg):
         arr = (capi.HbSystem * len(systems))()

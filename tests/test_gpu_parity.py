@@ -353,3 +353,24 @@ def test_autotune_picks_a_schedule_and_keeps_results(cuda):
     after = torch.empty_like(x)
     plan.sense_normal(x, after, sm, packed)
     assert torch.equal(before, after)
+
+
+def test_cg_host_buffers_match_device_cg(cuda):
+    """cg_host (host buffers, copies overlapped with the solves of other groups) gives the
+    device CG's result bit for bit."""
+    shape = (16, 16, 16)
+    coords, x, sm, T = _case(shape, 3, 600, 31)
+    plan = ToeplitzPlan(shape, cuda)
+    packed = plan.pack_diagonal(_c64(T, cuda))
+    rng = np.random.default_rng(32)
+    b = (rng.standard_normal((5,) + shape) + 1j * rng.standard_normal((5,) + shape)).astype(np.complex64)
+    xd = torch.zeros((5,) + shape, dtype=torch.complex64, device=cuda)
+    plan.cg(xd, torch.from_numpy(b).to(cuda), _c64(sm, cuda), packed, iters=6, lam=1e-2)
+    xh = torch.zeros((5,) + shape, dtype=torch.complex64).pin_memory()
+    out = torch.empty_like(xh).pin_memory()
+    st, it = plan.cg_host(xh, torch.from_numpy(b).pin_memory(), _c64(sm, cuda), packed, iters=6, lam=1e-2, chunks=3,
+                          out_host=out)
+    torch.cuda.synchronize()
+    assert it == [6] * 5
+    assert torch.equal(out, xd.cpu())
+    assert float(xh.abs().max()) == 0.0  # the initial guess is read, not overwritten
