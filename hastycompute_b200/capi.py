@@ -19,6 +19,8 @@ HB_ERR_WORKSPACE = 4
 HB_ERR_NOT_PD = 5
 
 HB_NOALLOC_SCRATCH_BYTES = 16 << 20
+HB_PRECISION_FP32 = 0
+HB_PRECISION_BF16X3 = 1
 
 HB_CG_RUNNING = 0
 HB_CG_CONVERGED = 1
@@ -52,6 +54,9 @@ SIGNATURES = {
     "hb_size_supported": (c_int, [c_i64, c_i64, c_i64]),
     "hb_plan_create": (c_int, [ctypes.POINTER(c_void_p), c_i64, c_i64, c_i64, c_int]),
     "hb_plan_destroy": (c_int, [c_void_p]),
+    "hb_plan_set_precision": (c_int, [c_void_p, c_int]),
+    "hb_plan_precision": (c_int, [c_void_p]),
+    "hb_wait_status": (c_int, [c_int]),
     "hb_diag_packed_floats": (c_i64, [c_void_p]),
     "hb_diag_pack": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "hb_diag_build_workspace_bytes": (c_size, [c_void_p, c_i64]),

@@ -15,6 +15,7 @@
 #include "diag_kernels.cuh"
 #include "fft3_launch.cuh"
 #include "runtime.cuh"
+#include "tc_kernels.cuh"
 #include "toeplitz_kernels.cuh"
 
 using namespace hb;
@@ -25,6 +26,9 @@ struct hb_plan {
   float2* tables;  // device twiddle tables (table_offsets layout)
   TableOffsets to;
   int plane_variant = -1;  // plane-pass schedule chosen by hb_plan_autotune (-1: default)
+  int precision = HB_PRECISION_FP32;
+  unsigned char* tc_ftab = nullptr;  // tensor-core pass A: DFT rows in operand layout
+  int* tc_wait_error = nullptr;      // device address of g_tc_wait_error
 };
 
 namespace hb {
@@ -78,6 +82,57 @@ cudaError_t ensure_smem(size_t bytes) {
 
 // ---------------------------------------------------------------- pass launchers ----
 using PassLauncher = cudaError_t (*)(const PassArgs&, int, cudaStream_t);
+
+// Set by the tensor-core pass when an mbarrier wait gave up (read and cleared by
+// hb_wait_status).
+__device__ int g_tc_wait_error;
+
+cudaError_t launch_a_tc(const hb_plan* p, const PassArgs& a, cudaStream_t st) {
+  cudaError_t e = ensure_smem<expand_fwd_x_tc_kernel<128>>(tc::kSmemBytes);
+  if (e != cudaSuccess) return e;
+  dim3 grid(2, a.N0, a.nslots);
+  LaunchScope ls(HB_KERNEL_EXPAND_FWD_X, st);
+  expand_fwd_x_tc_kernel<128><<<grid, tc::kThreads, tc::kSmemBytes, st>>>(a, p->tc_ftab, p->tc_wait_error);
+  return cudaGetLastError();
+}
+
+uint16_t bf16_bits_rn(float f) {  // round to nearest even (finite inputs)
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+double bf16_value(uint16_t b) {
+  const uint32_t u = (uint32_t)b << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return (double)f;
+}
+
+// Forward DFT rows F[kx][x] = exp(-2 pi i kx x / M2) (kx < M2, x < N2) in the tensor-core
+// pass's operand layout: [kx half][16-sample chunk][re_hi, re_lo, im_hi, im_lo] blocks of
+// tc::kArr bytes, element (kx, x) at tc::operand_offset(kx % 128, x % 16); hi = bf16(v),
+// lo = bf16(v - hi), v in FP64.
+std::vector<uint16_t> tc_dft_table(int N2) {
+  const int M2 = 2 * N2, nch = N2 / tc::kKc;
+  const size_t arr = tc::kArr / 2;  // uint16 per array
+  std::vector<uint16_t> t((size_t)(M2 / tc::kCols) * nch * 4 * arr);
+  for (int kx = 0; kx < M2; ++kx)
+    for (int x = 0; x < N2; ++x) {
+      const long long m = ((long long)kx * x) % M2;
+      const double ang = -2.0 * M_PI * (double)m / (double)M2;
+      const double v[2] = {std::cos(ang), std::sin(ang)};
+      const size_t blk = (size_t)(kx / tc::kCols) * nch + x / tc::kKc;
+      const size_t off = (size_t)tc::operand_offset(kx % tc::kCols, x % tc::kKc) / 2;
+      for (int c = 0; c < 2; ++c) {
+        const uint16_t hi = bf16_bits_rn((float)v[c]);
+        const uint16_t lo = bf16_bits_rn((float)(v[c] - bf16_value(hi)));
+        t[(blk * 4 + 2 * c) * arr + off] = hi;
+        t[(blk * 4 + 2 * c + 1) * arr + off] = lo;
+      }
+    }
+  return t;
+}
 
 template <int N2, int YT>
 cudaError_t launch_a(const PassArgs& a, int nsys, cudaStream_t st) {
@@ -239,7 +294,7 @@ int run_normal(const hb_plan* p, PassArgs a, cudaStream_t st) {
   const int ia = axis_index(p->N2), iy = ilog2(yt) - 3;
   const int nslots = a.nslots;
   if (nslots > 65535) return fail(HB_ERR_INVALID, "too many system x coil slots in one launch (max 65535)");
-  cudaError_t e = kLaunchA[ia][iy](a, a.nsys, st);
+  cudaError_t e = p->precision == HB_PRECISION_BF16X3 ? launch_a_tc(p, a, st) : kLaunchA[ia][iy](a, a.nsys, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass A: ") + cudaGetErrorString(e));
   e = plane_launcher(p)(a, nslots, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass B: ") + cudaGetErrorString(e));
@@ -773,7 +828,50 @@ int hb_plan_destroy(hb_plan* p) {
   if (!p) return HB_OK;
   DeviceGuard dg(p->device);
   if (p->tables) cudaFree(p->tables);
+  if (p->tc_ftab) cudaFree(p->tc_ftab);
   delete p;
+  return HB_OK;
+}
+
+int hb_plan_set_precision(hb_plan* p, int precision) {
+  if (int r = check_plan(p)) return r;
+  if (precision == HB_PRECISION_FP32) {
+    p->precision = precision;
+    return HB_OK;
+  }
+  if (precision != HB_PRECISION_BF16X3) return fail(HB_ERR_INVALID, "hb_plan_set_precision: unknown precision");
+  if (p->N1 != 128 || p->N2 != 128)
+    return fail(HB_ERR_UNSUPPORTED, "HB_PRECISION_BF16X3 needs ny = nx = 128 (tensor-core x pass), got ny = " +
+                                        std::to_string(p->N1) + ", nx = " + std::to_string(p->N2));
+  DeviceGuard dg(p->device);
+  if (!p->tc_ftab) {
+    const std::vector<uint16_t> t = tc_dft_table(p->N2);
+    cudaError_t e = cudaMalloc(&p->tc_ftab, t.size() * sizeof(uint16_t));
+    if (e == cudaSuccess) e = cudaMemcpy(p->tc_ftab, t.data(), t.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p->tc_wait_error, g_tc_wait_error);
+    if (e != cudaSuccess) {
+      if (p->tc_ftab) cudaFree(p->tc_ftab);
+      p->tc_ftab = nullptr;
+      return fail(HB_ERR_CUDA, std::string("tensor-core tables: ") + cudaGetErrorString(e));
+    }
+  }
+  p->precision = precision;
+  return HB_OK;
+}
+
+int hb_plan_precision(const hb_plan* p) { return p ? p->precision : -1; }
+
+int hb_wait_status(int device) {
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(HB_ERR_CUDA, "cannot select device " + std::to_string(device));
+  int flag = 0;
+  const int zero = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&flag, g_tc_wait_error, sizeof(int));
+  if (e == cudaSuccess && flag) e = cudaMemcpyToSymbol(g_tc_wait_error, &zero, sizeof(int));
+  if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("hb_wait_status: ") + cudaGetErrorString(e));
+  if (flag)
+    return fail(HB_ERR_CUDA, "a tensor-core pass gave up waiting for its operands or contractions (about 1 s); "
+                             "its output is incomplete");
   return HB_OK;
 }
 

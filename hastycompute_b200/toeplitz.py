@@ -61,7 +61,7 @@ class System:
 class ToeplitzPlan:
     """Geometry of an nz x ny x nx image and its 2x Toeplitz grid on one CUDA device."""
 
-    def __init__(self, nmodes, device=None):
+    def __init__(self, nmodes, device=None, precision="fp32"):
         self.lib = capi.load()
         if len(nmodes) == 4:  # reference convention [ntransf, nz, ny, nx]
             if nmodes[0] != 1:
@@ -77,6 +77,8 @@ class ToeplitzPlan:
         capi.check(self.lib.hb_plan_create(ctypes.byref(h), *self.shape, idx))
         self._h = h
         self._ws = None
+        if precision != "fp32":
+            self.set_precision(precision)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -86,6 +88,26 @@ class ToeplitzPlan:
             except Exception:
                 pass
             self._h = None
+
+    _PRECISIONS = {"fp32": capi.HB_PRECISION_FP32, "bf16x3": capi.HB_PRECISION_BF16X3}
+
+    def set_precision(self, precision):
+        """"fp32" (default): every pass on the CUDA cores in FP32.  "bf16x3": the forward x
+        pass as a tensor-core contraction with BF16 hi + lo operands and FP32 accumulation
+        (ny = nx = 128 only); the other passes stay FP32."""
+        if precision not in self._PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(self._PRECISIONS)}, got {precision!r}")
+        capi.check(self.lib.hb_plan_set_precision(self._h, self._PRECISIONS[precision]))
+
+    @property
+    def precision(self):
+        code = int(self.lib.hb_plan_precision(self._h))
+        return {v: k for k, v in self._PRECISIONS.items()}[code]
+
+    def wait_status(self):
+        """Raises if a tensor-core pass on this device gave up waiting (its output is then
+        incomplete); clears the flag.  Synchronous."""
+        capi.check(self.lib.hb_wait_status(self.device.index))
 
     @property
     def grid(self):

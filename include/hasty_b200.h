@@ -68,6 +68,25 @@ int hb_size_supported(int64_t nz, int64_t ny, int64_t nx);
 int hb_plan_create(hb_plan** plan, int64_t nz, int64_t ny, int64_t nx, int device);
 int hb_plan_destroy(hb_plan* plan);
 
+/* Arithmetic of the normal operator's x-axis pass.  No counterpart in the reference (its
+ * transforms are cuFFT in FP32).
+ *  HB_PRECISION_FP32   (default) every pass in FP32 on the CUDA cores.
+ *  HB_PRECISION_BF16X3 the forward x pass (coil expand, zero-pad, 2nx-point DFT) as a
+ *                      dense contraction on the tensor cores (tcgen05): BF16 hi + lo parts
+ *                      of both operands, three products per real product, FP32
+ *                      accumulation; the other passes stay FP32.  ny = nx = 128 only
+ *                      (HB_ERR_UNSUPPORTED otherwise).  Uploads a 256 KB table once.
+ * The setting applies to every later call with this plan. */
+#define HB_PRECISION_FP32 0
+#define HB_PRECISION_BF16X3 1
+int hb_plan_set_precision(hb_plan* plan, int precision);
+int hb_plan_precision(const hb_plan* plan);
+
+/* Reads and clears the device's flag for a tensor-core pass that gave up waiting on one
+ * of its mbarriers (after about one second): HB_ERR_CUDA with a message if it was set
+ * (the output of that launch is incomplete), else HB_OK.  Synchronous. */
+int hb_wait_status(int device);
+
 /* Number of floats of one packed diagonal (= 8 * nz * ny * nx). */
 int64_t hb_diag_packed_floats(const hb_plan* plan);
 
