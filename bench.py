@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--rates", default="1,2,4", help="serve: arrival rates (jobs/s)")
     ap.add_argument("--duration", type=float, default=30.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3"],
+                    help="batch mode: fp32 everywhere, or the forward x pass as a BF16 hi+lo tensor-core "
+                         "contraction (the reduced-precision plan)")
     ap.add_argument("--diag", default="nufft", choices=["nufft", "exact"],
                     help="Toeplitz diagonal construction: the reference's NUFFT route (tol 1e-6) or FP64-exact")
     return ap.parse_args()
@@ -395,6 +398,23 @@ def main():
     plan.sense_normal(xtrue, b, sm, packed, diag_index=diag_index, lam=a.lam)
     x = torch.zeros_like(b)
     torch.cuda.synchronize()
+    precision_check = None
+    if a.precision != "fp32":
+        # the right-hand side stays the FP32 one; the solves run on the reduced-precision plan,
+        # checked against the FP32 plan on the same inputs (one apply of two systems, and the
+        # CG solution of every system after the timed steps)
+        plan.set_precision(a.precision)
+        ref_plan = ToeplitzPlan(shape, dev)
+        nchk = min(2, nsys)
+        o_rp = torch.empty_like(xtrue[:nchk])
+        o_fp = torch.empty_like(xtrue[:nchk])
+        plan.sense_normal(xtrue[:nchk], o_rp, sm, packed, diag_index=diag_index[:nchk], lam=a.lam)
+        ref_plan.sense_normal(xtrue[:nchk], o_fp, sm, packed, diag_index=diag_index[:nchk], lam=a.lam)
+        plan.wait_status()
+        precision_check = {"apply_rel_l2_vs_fp32": max(
+            (torch.linalg.vector_norm(o_rp[i] - o_fp[i]) / torch.linalg.vector_norm(o_fp[i])).item()
+            for i in range(nchk))}
+        del o_rp, o_fp
 
     def step():
         x.zero_()
@@ -429,6 +449,14 @@ def main():
         ms = float(t.item())
     applies_per_step = nsys * (a.iters + 1)
     value = world * applies_per_step * a.steps / (ms / 1000.0)
+    if precision_check is not None:
+        x_rp = x.clone()
+        x.zero_()
+        ref_plan.cg(x, b, sm, packed, iters=a.iters, lam=a.lam, diag_index=diag_index)
+        plan.wait_status()
+        precision_check["cg_solution_max_rel_l2_vs_fp32"] = max(
+            (torch.linalg.vector_norm(x_rp[i] - x[i]) / torch.linalg.vector_norm(x[i])).item() for i in range(nsys))
+        del x_rp, ref_plan
 
     # ---- end to end through the public API with host buffers ----
     e2e = None
@@ -505,7 +533,10 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": max(3, a.warmup), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic (seeded)", "config": workload_config(a),
+            "vs_baseline": None, "data": "synthetic (seeded)", "config": workload_config(a),
+            "dtype": "c64 (fp32)" if a.precision == "fp32" else
+                     "c64 (fp32; forward x pass bf16 hi+lo x3 on tensor cores, fp32 accumulation)",
+            "precision": a.precision, "precision_check": precision_check,
             "cg_solves_per_s": value / (a.iters + 1), "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "apply_yardstick": yard, "kernels": per_kernel, "cpu_baseline": cpu,
             "clocks": clk, "setup_s": {"diagonals": t_diag, "diagonal_method": a.diag},

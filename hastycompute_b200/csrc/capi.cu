@@ -92,7 +92,7 @@ cudaError_t launch_a_tc(const hb_plan* p, const PassArgs& a, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   dim3 grid(2, a.N0, a.nslots);
   LaunchScope ls(HB_KERNEL_EXPAND_FWD_X, st);
-  expand_fwd_x_tc_kernel<128><<<grid, tc::kThreads, tc::kSmemBytes, st>>>(a, p->tc_ftab, p->tc_wait_error);
+  expand_fwd_x_tc_kernel<128><<<grid, tc::kThreadsAll, tc::kSmemBytes, st>>>(a, p->tc_ftab, p->tc_wait_error);
   return cudaGetLastError();
 }
 

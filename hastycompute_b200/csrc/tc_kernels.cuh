@@ -11,12 +11,14 @@
 // memory, 256 columns per CTA, so two CTAs share an SM and one CTA's epilogue overlaps the
 // other's contraction.
 //
-// K runs in chunks of 16 samples (one instruction deep) through a ring of kStages stages:
-// the threads split their chunk of A into the canonical K-major layout while the tensor
-// core contracts the previous chunk; the matching 16 KB of the constant F table (already
-// in that layout, hi/lo split on the host) arrives by one bulk copy (not multicast) that
-// completes on the stage's "full" mbarrier, and tcgen05.commit signals the stage's "done"
-// mbarrier when the contraction that read it has finished.  Every wait on an mbarrier
+// K runs in chunks of 16 samples (one instruction deep).  Warps 0-7 split chunk kc of A
+// into the canonical K-major layout (ring of kStagesA slots; the samples of chunk kc + 1
+// are loaded meanwhile) and arrive on the slot's "ready" mbarrier, while the tensor core
+// contracts chunk kc - 1.  One lane of warp 8 streams the constant F table (already in
+// that layout, hi/lo split on the host) by bulk copies (not multicast), kFAhead chunks
+// early into a ring of kStagesF slots with a "full" mbarrier each, waits for "ready" and
+// "full", issues the chunk's contractions and commits them to the chunk's "done"
+// mbarrier, which frees both slots.  Every wait on an mbarrier
 // gives up after about a second of SM clocks, sets the caller's error word and lets the
 // CTA release its tensor memory and return.
 //
@@ -39,11 +41,15 @@ constexpr int kKc = 16;                    // MMA K: x samples per chunk
 constexpr int kArr = kRows * kKc * 2;      // bytes of one BF16 operand array [128][16]
 constexpr int kStageA = 4 * kArr;          // A: re_hi, re_lo, im_hi, im_lo
 constexpr int kStageF = 4 * kArr;          // F: re_hi, re_lo, im_hi, im_lo
-constexpr int kStage = kStageA + kStageF;  // 32 KB
-constexpr int kStages = 3;
-constexpr int kThreads = 256;
+constexpr int kStagesA = 2;                // A slot of chunk kc is refilled by chunk kc + 2
+constexpr int kStagesF = 4;                // F slot of chunk kc is refilled by chunk kc + 4
+constexpr int kFAhead = 2;                 // F copies run this many chunks ahead
+constexpr int kDone = kStagesF;            // "done" mbarrier of chunk kc: kc % kDone
+constexpr int kThreads = 256;             // operand warps 0-7 (preparation, epilogue)
+constexpr int kThreadsAll = kThreads + 32;  // + warp 8: bulk copies and contractions
 constexpr int kTmemCols = 2 * kCols;       // D_re [0, 128), D_im [128, 256)
-constexpr int kSmemBytes = kStages * kStage;
+constexpr int kSmemBytes = kStagesA * kStageA + kStagesF * kStageF;  // 96 KB
+static_assert(kFAhead + kStagesA <= kStagesF, "the F slot refilled at chunk kc was freed by chunk kc - kStagesA");
 constexpr long long kWaitCycles = 2000000000LL;  // about one second of SM clocks
 
 // Byte offset of element (row r, k) in a [128][16] K-major operand array without swizzle:
@@ -92,21 +98,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Waits for the phase of the given parity to complete; false after kWaitCycles.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Waits for the phase of the given parity to complete; false after kWaitCycles or once
+// another thread of the CTA has raised *abort.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* abort) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity))
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (*abort || clock64() - t0 > kWaitCycles) return false;
   return true;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
-__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
-  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
-               : "memory");
+__device__ __forceinline__ void st_shared_b32(uint32_t addr, uint32_t v) {
+  asm volatile("st.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
@@ -135,33 +144,24 @@ __device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t adesc, uint64_t bd
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
-// 32 consecutive columns of this warp's 32 lanes, one lane per thread
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+// 16 consecutive columns of this warp's 32 lanes, one lane per thread
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// hi = bf16(v), lo = bf16(v - hi) for 8 values, packed in K order (element 2i in the low half)
-__device__ __forceinline__ void split_bf16x8(const float* v, uint4& hi, uint4& lo) {
-  uint32_t h[4], l[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-    const float2 pf = __bfloat1622float2(p);
-    const __nv_bfloat162 q = __floats2bfloat162_rn(v[2 * i] - pf.x, v[2 * i + 1] - pf.y);
-    h[i] = *reinterpret_cast<const uint32_t*>(&p);
-    l[i] = *reinterpret_cast<const uint32_t*>(&q);
-  }
-  hi = make_uint4(h[0], h[1], h[2], h[3]);
-  lo = make_uint4(l[0], l[1], l[2], l[3]);
+// hi = bf16(v), lo = bf16(v - hi) for 2 values, packed in K order (v[0] in the low half)
+__device__ __forceinline__ void split_bf16x2(const float* v, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 p = __floats2bfloat162_rn(v[0], v[1]);
+  const float2 pf = __bfloat1622float2(p);
+  const __nv_bfloat162 q = __floats2bfloat162_rn(v[0] - pf.x, v[1] - pf.y);
+  hi = *reinterpret_cast<const uint32_t*>(&p);
+  lo = *reinterpret_cast<const uint32_t*>(&q);
 }
 
 }  // namespace tc
@@ -170,16 +170,18 @@ __device__ __forceinline__ void split_bf16x8(const float* v, uint4& hi, uint4& l
 // im_lo][operand_offset] BF16 (kStageF bytes per (half, chunk)); wait_error: set to 1 when
 // an mbarrier wait gave up.
 template <int N2>
-__global__ void __launch_bounds__(tc::kThreads, 2) expand_fwd_x_tc_kernel(PassArgs a, const unsigned char* ftab,
-                                                                          int* wait_error) {
+__global__ void __launch_bounds__(tc::kThreadsAll, 2) expand_fwd_x_tc_kernel(PassArgs a, const unsigned char* ftab,
+                                                                             int* wait_error) {
   using namespace tc;
   static_assert(N2 == 128, "tensor-core x pass: nx = 128");
   constexpr int M2 = 2 * N2, NCH = N2 / kKc;
-  extern __shared__ float2 smem[];  // operand stages (16-byte aligned, checked below)
-  __shared__ __align__(8) uint64_t bar_full[kStages];
-  __shared__ __align__(8) uint64_t bar_done[kStages];
+  extern __shared__ float2 smem[];  // A ring, then F ring (16-byte aligned, checked below)
+  __shared__ __align__(8) uint64_t bar_full[kStagesF];   // F slot landed (bulk copy)
+  __shared__ __align__(8) uint64_t bar_ready[kStagesA];  // A slot written (kThreads arrivals)
+  __shared__ __align__(8) uint64_t bar_done[kDone];      // chunk contracted (tcgen05.commit)
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
+  volatile int* abort = &abort_sh;
 
   const int h = blockIdx.x, z = blockIdx.y, slot = blockIdx.z;
   const int sys = a.slot_sys[slot];
@@ -191,13 +193,13 @@ __global__ void __launch_bounds__(tc::kThreads, 2) expand_fwd_x_tc_kernel(PassAr
     if (tid == 0) atomicExch(wait_error, 1);
     return;
   }
+  const uint32_t sF = sbase + kStagesA * kStageA;
 
   if (warp == 0) tmem_alloc(smem_u32(&tmem_sh), kTmemCols);
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(smem_u32(&bar_full[s]), 1);
-      mbar_init(smem_u32(&bar_done[s]), 1);
-    }
+    for (int s = 0; s < kStagesF; ++s) mbar_init(smem_u32(&bar_full[s]), 1);
+    for (int s = 0; s < kStagesA; ++s) mbar_init(smem_u32(&bar_ready[s]), kThreads);
+    for (int s = 0; s < kDone; ++s) mbar_init(smem_u32(&bar_done[s]), 1);
     fence_mbar_init();
     abort_sh = 0;
   }
@@ -205,71 +207,38 @@ __global__ void __launch_bounds__(tc::kThreads, 2) expand_fwd_x_tc_kernel(PassAr
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_sh;
+  auto done_wait = [&](int c) { return mbar_wait(smem_u32(&bar_done[c % kDone]), (c / kDone) & 1, abort); };
 
-  const long long plane = (long long)N1 * N2;
-  const float2* xs = a.sys_x[sys] + (long long)z * plane;
-  const float2* sm = a.sys_smaps[sys];
-  const float2* ss = sm ? sm + ((long long)a.slot_coil[slot] * N0 + z) * plane : nullptr;
-  // operand preparation: thread -> row y = pr, 8-sample K half pg of each chunk
-  const int pr = tid % kRows, pg = tid / kRows;
-  const uint32_t poff = (uint32_t)operand_offset(pr, 8 * pg);
-
-  int committed = -1;  // last chunk whose contraction was committed (thread 0)
-  int pending = -1;    // chunk whose F copy was issued and not yet seen complete (thread 0)
+  if (warp == kThreads / 32) {
+    if (lane == 0) {
+      // ---- issuer: F table copies and the contractions ----
+      auto issue_f = [&](int c) {
+        const int fs = c % kStagesF;
+        mbar_expect_tx(smem_u32(&bar_full[fs]), kStageF);
+        bulk_copy_g2s(sF + fs * kStageF, ftab + (size_t)(h * NCH + c) * kStageF, kStageF, smem_u32(&bar_full[fs]));
+      };
+      int committed = -1, issued_f = -1, landed_f = -1;
+      bool ok = true;
+      for (int c = 0; c < kFAhead && c < NCH; ++c) issue_f(issued_f = c);
 #pragma unroll 1
-  for (int kc = 0; kc < NCH; ++kc) {
-    const int s = kc % kStages, use = kc / kStages;
-    const uint32_t st = sbase + s * kStage;
-    if (tid == 0) {
-      // the contraction that last read stage s has finished
-      if (kc >= kStages && !mbar_wait(smem_u32(&bar_done[s]), (use - 1) & 1)) abort_sh = 1;
-      if (!abort_sh) {
-        mbar_expect_tx(smem_u32(&bar_full[s]), kStageF);
-        bulk_copy_g2s(st + kStageA, ftab + (size_t)(h * NCH + kc) * kStageF, kStageF, smem_u32(&bar_full[s]));
-        pending = kc;
-      }
-    }
-    __syncthreads();
-    if (abort_sh) break;
-    {
-      // 8-byte loads: a system's image and coil maps need only complex64 alignment
-      const int x0 = kc * kKc + 8 * pg;
-      const float2* xp = xs + (long long)pr * N2 + x0;
-      float re[8], im[8];
-      float2 xv[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) xv[i] = __ldg(xp + i);
-      if (ss) {
-        const float2* sp = ss + (long long)pr * N2 + x0;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) xv[i] = cmul(xv[i], __ldg(sp + i));
-      }
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        re[i] = xv[i].x;
-        im[i] = xv[i].y;
-      }
-      uint4 rh, rl, ih, il;
-      split_bf16x8(re, rh, rl);
-      split_bf16x8(im, ih, il);
-      st_shared_v4(st + 0 * kArr + poff, rh);
-      st_shared_v4(st + 1 * kArr + poff, rl);
-      st_shared_v4(st + 2 * kArr + poff, ih);
-      st_shared_v4(st + 3 * kArr + poff, il);
-    }
-    fence_proxy_async_smem();  // the generic-proxy stores become visible to the tensor core
-    __syncthreads();
-    if (tid == 0) {
-      if (!mbar_wait(smem_u32(&bar_full[s]), use & 1)) {
-        abort_sh = 1;
-      } else {
-        pending = -1;
+      for (int kc = 0; kc < NCH && ok; ++kc) {
+        if (kc + kFAhead < NCH) {
+          const int prev = kc + kFAhead - kStagesF;  // last user of that F slot
+          if (prev >= 0 && !done_wait(prev)) { ok = false; break; }
+          issue_f(issued_f = kc + kFAhead);
+        }
+        if (!mbar_wait(smem_u32(&bar_ready[kc % kStagesA]), (kc / kStagesA) & 1, abort) ||
+            !mbar_wait(smem_u32(&bar_full[kc % kStagesF]), (kc / kStagesF) & 1, abort)) {
+          ok = false;
+          break;
+        }
+        landed_f = kc;
         tc_fence_after();
-        const uint32_t fb = st + kStageA;
-        const uint64_t A0 = smem_desc(st), A1 = smem_desc(st + kArr), A2 = smem_desc(st + 2 * kArr),
-                       A3 = smem_desc(st + 3 * kArr);
-        const uint64_t F0 = smem_desc(fb), F1 = smem_desc(fb + kArr), F2 = smem_desc(fb + 2 * kArr),
-                       F3 = smem_desc(fb + 3 * kArr);
+        const uint32_t sa = sbase + (kc % kStagesA) * kStageA, sf = sF + (kc % kStagesF) * kStageF;
+        const uint64_t A0 = smem_desc(sa), A1 = smem_desc(sa + kArr), A2 = smem_desc(sa + 2 * kArr),
+                       A3 = smem_desc(sa + 3 * kArr);
+        const uint64_t F0 = smem_desc(sf), F1 = smem_desc(sf + kArr), F2 = smem_desc(sf + 2 * kArr),
+                       F3 = smem_desc(sf + 3 * kArr);
         const uint32_t dre = tmem, dim = tmem + kCols;
         const uint32_t acc = kc > 0 ? 1u : 0u;
         // D_re += A_re F_re - A_im F_im
@@ -286,42 +255,110 @@ __global__ void __launch_bounds__(tc::kThreads, 2) expand_fwd_x_tc_kernel(PassAr
         mma_bf16(dim, A2, F0, kIdesc, 1u);
         mma_bf16(dim, A2, F1, kIdesc, 1u);
         mma_bf16(dim, A3, F0, kIdesc, 1u);
-        mma_commit(smem_u32(&bar_done[s]));
+        mma_commit(smem_u32(&bar_done[kc % kDone]));
         committed = kc;
+      }
+      if (!ok) abort_sh = 1;
+      // before the shared memory is released: every commit's arrival and every copy in
+      // flight has landed (bounded waits that ignore the abort flag)
+      const long long t0 = clock64();
+      for (int c = committed; c >= 0 && c > committed - kDone; --c)
+        while (!mbar_try_wait(smem_u32(&bar_done[c % kDone]), (c / kDone) & 1) && clock64() - t0 < kWaitCycles) {
+        }
+      for (int c = landed_f + 1; c <= issued_f; ++c)
+        while (!mbar_try_wait(smem_u32(&bar_full[c % kStagesF]), (c / kStagesF) & 1) && clock64() - t0 < kWaitCycles) {
+        }
+    }
+  } else {
+    // ---- operand warps: task j (< 4) of a thread is row r = 32 j + 4 warp + lane / 8 and
+    // the sample pair pp = lane % 8 of the chunk, so that one load instruction of a warp
+    // reads four 128-byte row segments; 16-byte loads when the image and the coil maps are
+    // 16-byte aligned, else 8-byte loads (complex64 alignment); the next chunk's samples
+    // are loaded while the current one is split ----
+    const long long plane = (long long)N1 * N2;
+    const float2* xs = a.sys_x[sys] + (long long)z * plane;
+    const float2* sm = a.sys_smaps[sys];
+    const float2* ss = sm ? sm + ((long long)a.slot_coil[slot] * N0 + z) * plane : nullptr;
+    const int pp = lane % 8, rbase = 4 * warp + lane / 8;
+    const bool vec = ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(ss)) & 15u) == 0;
+    float4 nx[4], ns[4];
+    auto ld2 = [&](const float2* q) {
+      if (vec) return __ldg(reinterpret_cast<const float4*>(q));
+      const float2 u = __ldg(q), v = __ldg(q + 1);
+      return make_float4(u.x, u.y, v.x, v.y);
+    };
+    auto load_chunk = [&](int kc) {
+      const int x0 = kc * kKc + 2 * pp;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const long long o = (long long)(rbase + 32 * j) * N2 + x0;
+        nx[j] = ld2(xs + o);
+        if (ss) ns[j] = ld2(ss + o);
+      }
+    };
+    load_chunk(0);
+    bool ok = true;
+#pragma unroll 1
+    for (int kc = 0; kc < NCH; ++kc) {
+      // the contraction of chunk kc - kStagesA, which read this A slot, has finished
+      if (kc >= kStagesA && !done_wait(kc - kStagesA)) {
+        ok = false;
+        break;
+      }
+      const uint32_t sa = sbase + (kc % kStagesA) * kStageA;
+      float re[4][2], im[4][2];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        float2 u = make_float2(nx[j].x, nx[j].y), v = make_float2(nx[j].z, nx[j].w);
+        if (ss) {
+          u = cmul(u, make_float2(ns[j].x, ns[j].y));
+          v = cmul(v, make_float2(ns[j].z, ns[j].w));
+        }
+        re[j][0] = u.x;
+        re[j][1] = v.x;
+        im[j][0] = u.y;
+        im[j][1] = v.y;
+      }
+      if (kc + 1 < NCH) load_chunk(kc + 1);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        uint32_t rh, rl, ih, il;
+        split_bf16x2(re[j], rh, rl);
+        split_bf16x2(im[j], ih, il);
+        const uint32_t off = sa + (uint32_t)operand_offset(rbase + 32 * j, 2 * pp);
+        st_shared_b32(off + 0 * kArr, rh);
+        st_shared_b32(off + 1 * kArr, rl);
+        st_shared_b32(off + 2 * kArr, ih);
+        st_shared_b32(off + 3 * kArr, il);
+      }
+      fence_proxy_async_smem();  // the generic-proxy stores become visible to the tensor core
+      mbar_arrive(smem_u32(&bar_ready[kc % kStagesA]));
+    }
+    if (ok) ok = done_wait(NCH - 1);  // the last commit covers every contraction
+    if (!ok) {
+      abort_sh = 1;
+    } else {
+      tc_fence_after();
+      // epilogue: warp w reads TMEM lanes [32 (w % 4), +32) = lines y, columns (kx) of half w / 4
+      const int q = warp % 4, ch = warp / 4;
+      const int y = q * 32 + lane;
+      float2* dst = a.spill + spill_offset(slot, z, h * kCols, N0, N1, M2) + y;
+#pragma unroll 1
+      for (int cb = 0; cb < 4; ++cb) {
+        const int c0 = ch * 64 + cb * 16;
+        uint32_t re[16], im[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, re);
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kCols + c0), im);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          dst[(long long)(c0 + j) * N1] = make_float2(__uint_as_float(re[j]), __uint_as_float(im[j]));
       }
     }
   }
-  if (tid == 0) {
-    // the last commit covers every contraction issued before it; the earlier commits'
-    // arrivals are awaited too, so that none lands after the CTA's shared memory is released
-    for (int c = committed; c >= 0 && c > committed - kStages; --c)
-      if (!mbar_wait(smem_u32(&bar_done[c % kStages]), (c / kStages) & 1)) abort_sh = 1;
-    // on an abort, a copy still in flight must land before the CTA's shared memory is released
-    if (pending >= 0) mbar_wait(smem_u32(&bar_full[pending % kStages]), (pending / kStages) & 1);
-  }
-  __syncthreads();
-  if (!abort_sh) {
-    tc_fence_after();
-    // epilogue: warp w reads TMEM lanes [32 (w % 4), +32) = lines y, columns (kx) of half w / 4
-    const int q = warp % 4, ch = warp / 4;
-    const int y = q * 32 + lane;
-    float2* dst = a.spill + spill_offset(slot, z, h * kCols, N0, N1, M2) + y;
-#pragma unroll 1
-    for (int cb = 0; cb < 2; ++cb) {
-      const int c0 = ch * 64 + cb * 32;
-      uint32_t re[32], im[32];
-      tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, re);
-      tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kCols + c0), im);
-      tmem_ld_wait();
-#pragma unroll
-      for (int j = 0; j < 32; ++j)
-        dst[(long long)(c0 + j) * N1] = make_float2(__uint_as_float(re[j]), __uint_as_float(im[j]));
-    }
-  } else if (tid == 0) {
-    atomicExch(wait_error, 1);
-  }
   tc_fence_before();
   __syncthreads();
+  if (tid == 0 && abort_sh) atomicExch(wait_error, 1);
   if (warp == 0) tmem_dealloc(tmem, kTmemCols);
 }
 
