@@ -103,3 +103,46 @@ def test_cg_matches_oracle(cuda, case):
         A = O.regularized(lambda v, s=s: O.sense_normal_toeplitz(v, sm, Ts[s]), lam)
         xo, _ = O.conjugate_gradient(A, bs[s], iters=iters)
         assert O.rel_l2(_np(xg[s]), xo) < TOL_ORACLE
+
+
+def test_unaligned_image_and_maps_take_the_narrow_loads(cuda, case):
+    """Images and coil maps only 8-byte aligned (complex64 views one element into a
+    buffer) go through the pass's 8-byte loads and give the same bits as aligned copies."""
+    Ts, sm, xs = case
+    plan = ToeplitzPlan(SHAPE, cuda, precision="bf16x3")
+    packed = plan.pack_diagonal(_c64(Ts[0], cuda))
+    n = int(np.prod(SHAPE))
+    xbuf = torch.zeros(n + 1, dtype=torch.complex64, device=cuda)
+    xbuf[1:] = _c64(xs[0], cuda).reshape(-1)
+    sbuf = torch.zeros(3 * n + 1, dtype=torch.complex64, device=cuda)
+    sbuf[1:] = _c64(sm, cuda).reshape(-1)
+    x_odd, s_odd = xbuf[1:].view(SHAPE), sbuf[1:].view((3,) + SHAPE)
+    assert x_odd.data_ptr() % 16 == 8 and s_odd.data_ptr() % 16 == 8
+    out_odd = torch.empty(SHAPE, dtype=torch.complex64, device=cuda)
+    out = torch.empty_like(out_odd)
+    plan.sense_normal(x_odd, out_odd, s_odd, packed)
+    plan.sense_normal(_c64(xs[0], cuda), out, _c64(sm, cuda), packed)
+    plan.wait_status()
+    assert torch.equal(out_odd, out)
+    assert O.rel_l2(_np(out), O.sense_normal_toeplitz(xs[0], sm, Ts[0])) < TOL_ORACLE
+
+
+def test_cg_systems_that_converge_early_are_skipped(cuda, case):
+    """One system converges in the first iterations (identity operator, unit-power maps)
+    while the other keeps iterating: later launches skip the converged system's slots."""
+    Ts, sm, xs = case
+    plan = ToeplitzPlan(SHAPE, cuda, precision="bf16x3")
+    T_id = np.ones(plan.grid, np.complex128)
+    packed = torch.cat([plan.pack_diagonal(_c64(T_id, cuda)), plan.pack_diagonal(_c64(Ts[1], cuda))])
+    # the second right-hand side is scaled so that its residual stays far above the
+    # (absolute) tolerance for all 6 iterations (oracle: 6.9 against 0.51 at the last)
+    bs = np.stack([xs[0], 1e5 * O.sense_normal_toeplitz(xs[1], sm, Ts[1])])
+    x = torch.zeros((2,) + SHAPE, dtype=torch.complex64, device=cuda)
+    status, done = plan.cg(x, _c64(bs, cuda), _c64(sm, cuda), packed, iters=6, tol=1e-3 * float(np.linalg.norm(bs[0])),
+                           diag_index=[0, 1])
+    plan.wait_status()
+    assert status[0] == capi.HB_CG_CONVERGED and done[0] <= 2 and done[1] == 6
+    assert O.rel_l2(_np(x[0]), xs[0]) < 1e-4
+    A = lambda v: O.sense_normal_toeplitz(v, sm, Ts[1])
+    xo, _ = O.conjugate_gradient(A, bs[1], iters=6)
+    assert O.rel_l2(_np(x[1]), xo) < TOL_ORACLE
