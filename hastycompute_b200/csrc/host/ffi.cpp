@@ -79,6 +79,9 @@ class BatchedSenseNormalToeplitz : public torch::CustomClassHolder {
     _op->apply(in, out, coils.has_value() ? *coils : all_coils(in), 0.0);
   }
 
+  // "fp32" (default) or "bf16x3" (forward x pass on the tensor cores, ny = nx = 128)
+  void set_precision(const std::string& name) { _op->plan()->set_precision(name); }
+
   void apply_regularized(const at::Tensor& in, at::Tensor out, double lambda,
                          const std::optional<std::vector<std::vector<int64_t>>>& coils) {
     _op->apply(in, out, coils.has_value() ? *coils : all_coils(in), lambda);
@@ -144,6 +147,7 @@ TORCH_LIBRARY(HastyToeplitz, m) {
       .def(torch::init<const at::Tensor&, const at::Tensor&, const std::optional<std::vector<int64_t>>&>())
       .def("apply", &hasty::ffi::BatchedSenseNormalToeplitz::apply)
       .def("apply_regularized", &hasty::ffi::BatchedSenseNormalToeplitz::apply_regularized)
+      .def("set_precision", &hasty::ffi::BatchedSenseNormalToeplitz::set_precision)
       .def("cg", &hasty::ffi::BatchedSenseNormalToeplitz::cg);
 
   m.def("batched_sense_toeplitz_diagonals", &hasty::ffi::batched_sense_toeplitz_diagonals);

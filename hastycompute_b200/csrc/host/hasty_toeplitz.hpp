@@ -20,6 +20,7 @@
 #include <memory>
 #include <optional>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 struct hb_plan;
@@ -43,6 +44,9 @@ class Plan {
   std::vector<int64_t> grid_dims() const { return {2 * _dims[0], 2 * _dims[1], 2 * _dims[2]}; }
   int64_t packed_numel() const;
   at::Tensor workspace(size_t bytes) const;  // device scratch from the caching allocator
+  // "fp32" (default) or "bf16x3": the forward x pass as a tensor-core contraction with
+  // BF16 hi + lo operands (ny = nx = 128); applies to every later call with this plan
+  void set_precision(const std::string& name);
 
  private:
   hb_plan* _p = nullptr;

@@ -34,6 +34,16 @@ Plan::~Plan() {
 
 int64_t Plan::packed_numel() const { return hb_diag_packed_floats(_p); }
 
+void Plan::set_precision(const std::string& name) {
+  if (name == "fp32") {
+    check(hb_plan_set_precision(_p, HB_PRECISION_FP32));
+  } else if (name == "bf16x3") {
+    check(hb_plan_set_precision(_p, HB_PRECISION_BF16X3));
+  } else {
+    throw std::runtime_error("precision must be \"fp32\" or \"bf16x3\", got \"" + name + "\"");
+  }
+}
+
 at::Tensor Plan::workspace(size_t bytes) const {
   return at::empty({(int64_t)std::max<size_t>(bytes, 1)}, at::TensorOptions().dtype(at::kByte).device(_device));
 }

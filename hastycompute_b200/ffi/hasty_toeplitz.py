@@ -60,6 +60,11 @@ class BatchedSenseNormalToeplitz:
         else:
             self._senseop.apply_regularized(input, output, float(lamda), coils)
 
+    def set_precision(self, precision):
+        """"fp32" (default) or "bf16x3": the forward x pass as a tensor-core contraction with
+        BF16 hi + lo operands and FP32 accumulation (ny = nx = 128)."""
+        self._senseop.set_precision(precision)
+
     def cg(self, x, b, iters=30, tol=0.0, lamda=0.0, coils=None):
         """ConjugateGradient on (A^H A)_toeplitz + lamda I for every outer batch of x (in place)."""
         return self._senseop.cg(x, b, int(iters), float(tol), float(lamda), coils)

@@ -88,6 +88,23 @@ def test_batched_sense_cpu_tensors_and_cg(ffi, cuda):
         assert O.rel_l2(_np(xs[i, 0]), xo) < 1e-4
 
 
+def test_batched_sense_reduced_precision_through_the_torchscript_class(ffi, cuda):
+    """set_precision("bf16x3") on the TorchScript class: the forward x pass runs on the
+    tensor cores (ny = nx = 128); the result stays within 1e-4 of the FP64 oracle."""
+    shape = (8, 128, 128)
+    rng = np.random.default_rng(4)
+    T = O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 200)), shape)
+    sm = synth.coil_maps(2, shape, seed=7)
+    op = ffi.BatchedSenseNormalToeplitz(torch.from_numpy(T[None].astype(np.complex64)), torch.from_numpy(sm), [0])
+    op.set_precision("bf16x3")
+    with pytest.raises(RuntimeError):
+        op.set_precision("fp16")
+    x = torch.from_numpy(synth.gaussian_image((1, 1) + shape, seed=8))
+    out = torch.empty_like(x)
+    op.apply(x, out, [[0, 1]])
+    assert O.rel_l2(out[0, 0].numpy(), O.sense_normal_toeplitz(x[0, 0].numpy(), sm, T, [0, 1])) < 1e-4
+
+
 def test_legacy_batched_binding_in_place(ffi, cuda):
     shape = (8, 8, 8)
     rng = np.random.default_rng(3)
