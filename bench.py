@@ -57,8 +57,8 @@ def parse():
     ap.add_argument("--duration", type=float, default=30.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3"],
-                    help="batch mode: fp32 everywhere, or the forward x pass as a BF16 hi+lo tensor-core "
-                         "contraction (the reduced-precision plan)")
+                    help="fp32 everywhere, or the forward x pass as a BF16 hi+lo tensor-core contraction (the "
+                         "reduced-precision plan; in the uneven and serve mixes for the 128^3 jobs)")
     ap.add_argument("--diag", default="nufft", choices=["nufft", "exact"],
                     help="Toeplitz diagonal construction: the reference's NUFFT route (tol 1e-6) or FP64-exact")
     return ap.parse_args()
@@ -210,6 +210,8 @@ def make_job_mix(a, dev, njobs, plans):
         spokes = int(rng.integers(1000, 4001))
         if shape not in plans:
             plans[shape] = ToeplitzPlan(shape, dev)
+            if a.precision != "fp32" and shape[1:] == (128, 128):  # tensor-core x pass: ny = nx = 128
+                plans[shape].set_precision(a.precision)
         plan = plans[shape]
         coords = torch.from_numpy(synth.kooshball(spokes, a.samples, frame=j % 7, nframes=7))
         try:
@@ -291,7 +293,8 @@ def run_uneven(a, dev):
     line = {
         "metric": "CG solves/s (uneven batch)", "value": nsys * a.steps / (ms / 1000.0), "unit": "solves/s",
         "applies_per_s": applies / (ms / 1000.0), "n_gpus": 1, "steps": a.steps, "warmup": 1,
-        "ms_per_step": ms / a.steps, "higher_is_better": True, "dtype": "c64 (fp32)", "data": "synthetic (seeded)",
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "data": "synthetic (seeded)", "precision": a.precision,
+        "dtype": "c64 (fp32)" if a.precision == "fp32" else "c64 (fp32; 128^3 jobs: forward x pass bf16 hi+lo x3)",
         "config": {"workload": f"{a.jobs} jobs, sizes {MIX_SHAPES}, coils {MIX_COILS}, 1-{a.max_frames} frames, "
                                f"1000-4000 spokes x {a.samples}, {a.iters}-iteration CG, one launch sequence per size "
                                f"class on its own stream, iterations replayed as CUDA graphs",
@@ -313,7 +316,8 @@ def run_serve(a, dev):
     rng = np.random.default_rng(a.seed + 1)
     results = []
     for rate in [float(r) for r in a.rates.split(",")]:
-        server = ReconServer(dev, hbm_budget_bytes=int(torch.cuda.mem_get_info(dev)[0] * 0.6), max_active=4)
+        server = ReconServer(dev, hbm_budget_bytes=int(torch.cuda.mem_get_info(dev)[0] * 0.6), max_active=4,
+                             precision=a.precision)
         # warm one job through the path
         j0 = pool[0]
         server.submit(ReconJob(j0["shape"], j0["smaps"], j0["packed"], [0] * j0["frames"], j0["b"],
@@ -341,7 +345,8 @@ def run_serve(a, dev):
                         "mean_s": st["mean_s"], "max_queue_wait_s": st["max_queue_wait_s"],
                         "solves_per_s": nsys / (t_end - t_start), "wall_s": t_end - t_start})
     line = {"metric": "p99 recon latency (served)", "value": max(r["p99_s"] for r in results), "unit": "s",
-            "higher_is_better": False, "n_gpus": 1, "dtype": "c64 (fp32)", "data": "synthetic (seeded)",
+            "higher_is_better": False, "n_gpus": 1, "data": "synthetic (seeded)", "precision": a.precision,
+            "dtype": "c64 (fp32)" if a.precision == "fp32" else "c64 (fp32; 128^3 jobs: forward x pass bf16 hi+lo x3)",
             "config": {"workload": f"Poisson arrivals, job pool of {a.jobs} as in the uneven mix, "
                                    f"{a.duration:.0f} s per rate, {a.iters}-iteration CG, admission by HBM footprint, "
                                    f"per-job streams (up to 4 concurrent)"},

@@ -114,7 +114,7 @@ class AdmissionQueue:
 
 
 class ReconServer:
-    def __init__(self, device=None, hbm_budget_bytes=None, max_active=4, graph=True):
+    def __init__(self, device=None, hbm_budget_bytes=None, max_active=4, graph=True, precision="fp32"):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if hbm_budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
@@ -122,6 +122,9 @@ class ReconServer:
         self.budget = int(hbm_budget_bytes)
         self.max_active = int(max_active)
         self.graph = graph
+        # "bf16x3": jobs with ny = nx = 128 run the forward x pass on the tensor cores
+        # (ToeplitzPlan.set_precision); other sizes stay FP32
+        self.precision = precision
         self._cv = threading.Condition()
         self._queue = AdmissionQueue(self.budget, self.max_active)
         self._closed = False
@@ -202,6 +205,8 @@ class ReconServer:
             stream = torch.cuda.Stream(self.device)
             # a plan per running job: plans keep a workspace cache, jobs must not share it
             plan = ToeplitzPlan(job.shape, self.device)
+            if self.precision != "fp32" and tuple(job.shape)[1:] == (128, 128):
+                plan.set_precision(self.precision)
             with torch.cuda.stream(stream):
                 nsys = len(job.frame_of_system)
                 x = torch.zeros((nsys,) + tuple(job.shape), dtype=torch.complex64, device=self.device)
