@@ -381,6 +381,7 @@ def main():
         pg = dist
 
     from hastycompute_b200 import capi, synth
+    from hastycompute_b200.replicas import job_rate, max_over_ranks, replica_seed
     from hastycompute_b200.toeplitz import ToeplitzPlan
 
     shape = (a.n,) * 3
@@ -398,7 +399,7 @@ def main():
     xtrue = torch.empty((nsys,) + shape, dtype=torch.complex64, device=dev)
     for f in range(a.frames):
         xtrue[f * a.encodings:(f + 1) * a.encodings] = torch.from_numpy(
-            synth.flow_phantom(shape, a.encodings, seed=100 + f)).to(dev)
+            synth.flow_phantom(shape, a.encodings, seed=replica_seed(100 + f, rank))).to(dev)
     b = torch.empty_like(xtrue)
     plan.sense_normal(xtrue, b, sm, packed, diag_index=diag_index, lam=a.lam)
     x = torch.zeros_like(b)
@@ -447,13 +448,9 @@ def main():
     if pg:
         pg.barrier()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    if pg:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), pg, dev)
     applies_per_step = nsys * (a.iters + 1)
-    value = world * applies_per_step * a.steps / (ms / 1000.0)
+    value = job_rate(world, applies_per_step * a.steps, ms)
     if precision_check is not None:
         x_rp = x.clone()
         x.zero_()
@@ -485,12 +482,8 @@ def main():
             e2e_step()
         e1.record()
         torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        if pg:
-            t = torch.tensor([ems], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": world * applies_per_step * a.steps / (ems / 1000.0), "unit": UNIT,
+        ems = max_over_ranks(e0.elapsed_time(e1), pg, dev)
+        e2e = {"value": job_rate(world, applies_per_step * a.steps, ems), "unit": UNIT,
                "h2d_bytes_per_step": int(xh.numel() * 8 + bh.numel() * 8), "d2h_bytes_per_step": int(outh.numel() * 8)}
 
     # ---- roofline of the dominant kernel ----
