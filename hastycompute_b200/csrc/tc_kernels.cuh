@@ -18,9 +18,10 @@
 // that layout, hi/lo split on the host) by bulk copies (not multicast), kFAhead chunks
 // early into a ring of kStagesF slots with a "full" mbarrier each, waits for "ready" and
 // "full", issues the chunk's contractions and commits them to the chunk's "done"
-// mbarrier, which frees both slots.  Every wait on an mbarrier
-// gives up after about a second of SM clocks, sets the caller's error word and lets the
-// CTA release its tensor memory and return.
+// mbarrier, which frees both slots.  Every wait on an mbarrier gives up after about a
+// second of SM clocks (or once another thread of the CTA has given up): the CTA then
+// drains its own copies and contractions, releases its tensor memory, sets the caller's
+// error word and returns without writing its output.
 //
 // No counterpart in the reference, which runs this transform through cuFFT
 // (lib/fft/nufft.cpp:1163-1197, fftn with s = 2N); the arithmetic is the transform's
