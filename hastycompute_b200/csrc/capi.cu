@@ -90,7 +90,7 @@ __device__ int g_tc_wait_error;
 cudaError_t launch_a_tc(const hb_plan* p, const PassArgs& a, cudaStream_t st) {
   cudaError_t e = ensure_smem<expand_fwd_x_tc_kernel<128>>(tc::kSmemBytes);
   if (e != cudaSuccess) return e;
-  dim3 grid(2, a.N0, a.nslots);
+  dim3 grid(a.N0, a.nslots);
   LaunchScope ls(HB_KERNEL_EXPAND_FWD_X, st);
   expand_fwd_x_tc_kernel<128><<<grid, tc::kThreadsAll, tc::kSmemBytes, st>>>(a, p->tc_ftab, p->tc_wait_error);
   return cudaGetLastError();
@@ -110,20 +110,20 @@ double bf16_value(uint16_t b) {
 }
 
 // Forward DFT rows F[kx][x] = exp(-2 pi i kx x / M2) (kx < M2, x < N2) in the tensor-core
-// pass's operand layout: [kx half][16-sample chunk][re_hi, re_lo, im_hi, im_lo] blocks of
-// tc::kArr bytes, element (kx, x) at tc::operand_offset(kx % 128, x % 16); hi = bf16(v),
+// pass's operand layout: [16-sample chunk][re_hi, re_lo, im_hi, im_lo] blocks of
+// tc::kArrF bytes, element (kx, x) at tc::operand_offset(kx, x % 16); hi = bf16(v),
 // lo = bf16(v - hi), v in FP64.
 std::vector<uint16_t> tc_dft_table(int N2) {
   const int M2 = 2 * N2, nch = N2 / tc::kKc;
-  const size_t arr = tc::kArr / 2;  // uint16 per array
-  std::vector<uint16_t> t((size_t)(M2 / tc::kCols) * nch * 4 * arr);
+  const size_t arr = tc::kArrF / 2;  // uint16 per array
+  std::vector<uint16_t> t((size_t)nch * 4 * arr);
   for (int kx = 0; kx < M2; ++kx)
     for (int x = 0; x < N2; ++x) {
       const long long m = ((long long)kx * x) % M2;
       const double ang = -2.0 * M_PI * (double)m / (double)M2;
       const double v[2] = {std::cos(ang), std::sin(ang)};
-      const size_t blk = (size_t)(kx / tc::kCols) * nch + x / tc::kKc;
-      const size_t off = (size_t)tc::operand_offset(kx % tc::kCols, x % tc::kKc) / 2;
+      const size_t blk = (size_t)(x / tc::kKc);
+      const size_t off = (size_t)tc::operand_offset(kx, x % tc::kKc) / 2;
       for (int c = 0; c < 2; ++c) {
         const uint16_t hi = bf16_bits_rn((float)v[c]);
         const uint16_t lo = bf16_bits_rn((float)(v[c] - bf16_value(hi)));

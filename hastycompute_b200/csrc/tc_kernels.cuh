@@ -3,13 +3,12 @@
 //
 //   spill[slot][z][kx][y] = sum_{x < nx} F[kx][x] * (S_c * x)[z][y][x],  F[kx][x] = e^{-2 pi i kx x / 2nx}
 //
-// One CTA per (slot, z, kx half): D^T[y][kx] = A[y][x] . F[kx][x]^T with A = S_c * x
-// (M = 128 lines y, N = 128 frequencies kx, K = 128 samples x).  Complex products are four
-// real products (the F_im terms of the real part through the instruction's negate-A bit).
-// Both operands are split into BF16 hi + lo parts and three products are kept per real
-// product (hi*hi + hi*lo + lo*hi); the accumulators D_re and D_im are FP32 in tensor
-// memory, 256 columns per CTA, so two CTAs share an SM and one CTA's epilogue overlaps the
-// other's contraction.
+// One CTA per (slot, z): D^T[y][kx] = A[y][x] . F[kx][x]^T with A = S_c * x (M = 128
+// lines y, N = 256 frequencies kx, K = 128 samples x), so every sample is loaded and split
+// once.  Complex products are four real products (the F_im terms of the real part through
+// the instruction's negate-A bit).  Both operands are split into BF16 hi + lo parts and
+// three products are kept per real product (hi*hi + hi*lo + lo*hi); the accumulators D_re
+// and D_im are FP32 in tensor memory (all 512 columns: one CTA per SM).
 //
 // K runs in chunks of 16 samples (one instruction deep).  Warps 0-7 split chunk kc of A
 // into the canonical K-major layout (ring of kStagesA slots; the samples of chunk kc + 1
@@ -37,34 +36,36 @@ namespace hb {
 namespace tc {
 
 constexpr int kRows = 128;                 // MMA M: y lines of one (slot, z) plane
-constexpr int kCols = 128;                 // MMA N: kx frequencies of one half
+constexpr int kCols = 256;                 // MMA N: kx frequencies (all of them)
 constexpr int kKc = 16;                    // MMA K: x samples per chunk
-constexpr int kArr = kRows * kKc * 2;      // bytes of one BF16 operand array [128][16]
+constexpr int kArr = kRows * kKc * 2;      // bytes of one BF16 A array [128][16]
+constexpr int kArrF = kCols * kKc * 2;     // bytes of one BF16 F array [256][16]
 constexpr int kStageA = 4 * kArr;          // A: re_hi, re_lo, im_hi, im_lo
-constexpr int kStageF = 4 * kArr;          // F: re_hi, re_lo, im_hi, im_lo
+constexpr int kStageF = 4 * kArrF;         // F: re_hi, re_lo, im_hi, im_lo
 constexpr int kStagesA = 2;                // A slot of chunk kc is refilled by chunk kc + 2
 constexpr int kStagesF = 4;                // F slot of chunk kc is refilled by chunk kc + 4
 constexpr int kFAhead = 2;                 // F copies run this many chunks ahead
 constexpr int kDone = kStagesF;            // "done" mbarrier of chunk kc: kc % kDone
 constexpr int kThreads = 256;             // operand warps 0-7 (preparation, epilogue)
 constexpr int kThreadsAll = kThreads + 32;  // + warp 8: bulk copies and contractions
-constexpr int kTmemCols = 2 * kCols;       // D_re [0, 128), D_im [128, 256)
-constexpr int kSmemBytes = kStagesA * kStageA + kStagesF * kStageF;  // 96 KB
+constexpr int kTmemCols = 2 * kCols;       // D_re [0, 256), D_im [256, 512)
+constexpr int kSmemBytes = kStagesA * kStageA + kStagesF * kStageF;  // 160 KB
 static_assert(kFAhead + kStagesA <= kStagesF, "the F slot refilled at chunk kc was freed by chunk kc - kStagesA");
 constexpr long long kWaitCycles = 2000000000LL;  // about one second of SM clocks
 
-// Byte offset of element (row r, k) in a [128][16] K-major operand array without swizzle:
+// Byte offset of element (row r, k) in a [rows][16] K-major operand array without swizzle:
 // core matrices of 8 rows x 16 bytes; the two 8-element K halves of an 8-row group are
 // adjacent (kLbo = 128 bytes apart, the descriptor's leading offset) and 8-row groups are
 // kSbo = 256 bytes apart (its stride offset).  With these two strides every address the
-// tensor core can form from the descriptor stays inside the 4 KB array whichever of the
-// two offsets it applies to which direction.
+// tensor core can form from the descriptor stays inside the array (4 KB for A, 8 KB for F)
+// whichever of the two offsets it applies to which direction.
 constexpr int kLbo = 128;
 constexpr int kSbo = 256;
 __host__ __device__ constexpr int operand_offset(int r, int k) {
   return (r / 8) * kSbo + (k / 8) * kLbo + (r % 8) * 16 + (k % 8) * 2;
 }
-static_assert(15 * kSbo + kLbo + 127 < kArr && 15 * kLbo + kSbo + 127 < kArr, "descriptor reach inside the array");
+static_assert(15 * kSbo + kLbo + 127 < kArr && 15 * kLbo + kSbo + 127 < kArr, "descriptor reach inside A");
+static_assert(31 * kSbo + kLbo + 127 < kArrF && 31 * kLbo + kSbo + 127 < kArrF, "descriptor reach inside F");
 
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bits 4-5 = 1), BF16
 // A and B (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24; bit 13
@@ -167,15 +168,16 @@ __device__ __forceinline__ void split_bf16x2(const float* v, uint32_t& hi, uint3
 
 }  // namespace tc
 
-// ftab: the forward DFT rows in operand layout, [kx half][chunk][re_hi, re_lo, im_hi,
-// im_lo][operand_offset] BF16 (kStageF bytes per (half, chunk)); wait_error: set to 1 when
-// an mbarrier wait gave up.
+// ftab: the forward DFT rows in operand layout, [chunk][re_hi, re_lo, im_hi,
+// im_lo][operand_offset] BF16 (kStageF bytes per chunk); wait_error: set to 1 when an
+// mbarrier wait gave up.
 template <int N2>
-__global__ void __launch_bounds__(tc::kThreadsAll, 2) expand_fwd_x_tc_kernel(PassArgs a, const unsigned char* ftab,
+__global__ void __launch_bounds__(tc::kThreadsAll, 1) expand_fwd_x_tc_kernel(PassArgs a, const unsigned char* ftab,
                                                                              int* wait_error) {
   using namespace tc;
   static_assert(N2 == 128, "tensor-core x pass: nx = 128");
   constexpr int M2 = 2 * N2, NCH = N2 / kKc;
+  static_assert(M2 == kCols, "one contraction covers every frequency kx");
   extern __shared__ float2 smem[];  // A ring, then F ring (16-byte aligned, checked below)
   __shared__ __align__(8) uint64_t bar_full[kStagesF];   // F slot landed (bulk copy)
   __shared__ __align__(8) uint64_t bar_ready[kStagesA];  // A slot written (kThreads arrivals)
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 2) expand_fwd_x_tc_kernel(Pas
   __shared__ int abort_sh;
   volatile int* abort = &abort_sh;
 
-  const int h = blockIdx.x, z = blockIdx.y, slot = blockIdx.z;
+  const int z = blockIdx.x, slot = blockIdx.y;
   const int sys = a.slot_sys[slot];
   if (a.active && !a.active[sys]) return;  // uniform for the CTA, before any allocation
   const int N0 = a.N0, N1 = a.N1;
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 2) expand_fwd_x_tc_kernel(Pas
       auto issue_f = [&](int c) {
         const int fs = c % kStagesF;
         mbar_expect_tx(smem_u32(&bar_full[fs]), kStageF);
-        bulk_copy_g2s(sF + fs * kStageF, ftab + (size_t)(h * NCH + c) * kStageF, kStageF, smem_u32(&bar_full[fs]));
+        bulk_copy_g2s(sF + fs * kStageF, ftab + (size_t)c * kStageF, kStageF, smem_u32(&bar_full[fs]));
       };
       int committed = -1, issued_f = -1, landed_f = -1;
       bool ok = true;
@@ -238,8 +240,8 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 2) expand_fwd_x_tc_kernel(Pas
         const uint32_t sa = sbase + (kc % kStagesA) * kStageA, sf = sF + (kc % kStagesF) * kStageF;
         const uint64_t A0 = smem_desc(sa), A1 = smem_desc(sa + kArr), A2 = smem_desc(sa + 2 * kArr),
                        A3 = smem_desc(sa + 3 * kArr);
-        const uint64_t F0 = smem_desc(sf), F1 = smem_desc(sf + kArr), F2 = smem_desc(sf + 2 * kArr),
-                       F3 = smem_desc(sf + 3 * kArr);
+        const uint64_t F0 = smem_desc(sf), F1 = smem_desc(sf + kArrF), F2 = smem_desc(sf + 2 * kArrF),
+                       F3 = smem_desc(sf + 3 * kArrF);
         const uint32_t dre = tmem, dim = tmem + kCols;
         const uint32_t acc = kc > 0 ? 1u : 0u;
         // D_re += A_re F_re - A_im F_im
@@ -343,10 +345,10 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 2) expand_fwd_x_tc_kernel(Pas
       // epilogue: warp w reads TMEM lanes [32 (w % 4), +32) = lines y, columns (kx) of half w / 4
       const int q = warp % 4, ch = warp / 4;
       const int y = q * 32 + lane;
-      float2* dst = a.spill + spill_offset(slot, z, h * kCols, N0, N1, M2) + y;
+      float2* dst = a.spill + spill_offset(slot, z, 0, N0, N1, M2) + y;
 #pragma unroll 1
-      for (int cb = 0; cb < 4; ++cb) {
-        const int c0 = ch * 64 + cb * 16;
+      for (int cb = 0; cb < kCols / 32; ++cb) {
+        const int c0 = ch * (kCols / 2) + cb * 16;
         uint32_t re[16], im[16];
         tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, re);
         tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kCols + c0), im);
