@@ -507,7 +507,7 @@ def main():
     dms = prof[dom][0] / max(1, prof[dom][1])
     achieved = alg[dom] / (dms / 1000.0) / 1e9
     # DRAM bytes (read + write) per (system, coil) slot of each pass, measured by ncu on one
-    # 16-coil system at 128^3 (profiles/passes_128c16_ncu_v3.md); a launch's traffic grows
+    # 16-coil system at 128^3 (the passes' ncu summary under profiles/); a launch's traffic grows
     # in proportion to its slots, so a full launch is that figure x slots
     traffic_per_slot = {"expand_fwd_x": 766.4e6 / 16, "plane_yz": 1084.0e6 / 16, "inv_x_combine": 839.6e6 / 16}
     traffic = traffic_per_slot[dom] * C * nsys if a.n == 128 else None

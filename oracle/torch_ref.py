@@ -1,7 +1,7 @@
 """The reference's LibTorch CPU path for the Toeplitz SENSE normal operator and CG,
 restated call for call with the same ATen operators (complex64, FP32).
 
-TEST / BASELINE INFRASTRUCTURE ONLY: used by ``tests/`` and by the CPU-baseline and
+TEST AND CPU-BASELINE INFRASTRUCTURE ONLY: used by ``tests/`` and by the CPU-baseline and
 ``--impl reference`` legs of ``bench.py``; never by the product path.
 
 The reference cannot be compiled here (C++20 header units, MSVC/clang-cl presets,
