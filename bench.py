@@ -516,6 +516,18 @@ def main():
                 "traffic_source": "ncu dram__bytes_read+write of one 16-slot launch, scaled by slots"
                 if traffic is not None else None,
                 "alg_bytes_per_launch": alg[dom], "ms_per_launch": dms}
+    # reduced-precision plan: tensor-pipe roofline of the tensor-core x pass.  Per (slot, z) it
+    # issues 8 chunks x 12 contractions of 128 x 256 x 16 (BF16 in, FP32 accumulate); a third
+    # of them carry the hi*hi products, the rest the hi*lo / lo*hi corrections
+    tensor_roofline = None
+    if a.precision != "fp32" and a.n == 128 and prof["expand_fwd_x"][1]:
+        ms_tc = prof["expand_fwd_x"][0] / prof["expand_fwd_x"][1]
+        flops = C * nsys * a.n * 8 * 12 * 2.0 * 128 * 256 * 16
+        peak_t = float(peaks.get("bf16_tflops_sustained", 1400.0))
+        tensor_roofline = {"bound": "tensor", "kernel": "expand_fwd_x_tc", "achieved": flops / (ms_tc / 1000.0) / 1e12,
+                           "peak": peak_t, "unit": "TFLOP/s", "frac": flops / (ms_tc / 1000.0) / 1e12 / peak_t,
+                           "peak_source": "measured (sustained bf16)" if "bf16_tflops_sustained" in peaks
+                           else "fallback", "flops_per_launch": flops, "ms_per_launch": ms_tc}
     # whole-apply yardstick: (18C + 10) * U bytes per normal-op apply
     b_alg = (18 * C + 10) * U
     apply_rate_dev = applies_per_step * a.steps / (ms / 1000.0)
@@ -534,7 +546,7 @@ def main():
             "vs_baseline": None, "data": "synthetic (seeded)", "config": workload_config(a),
             "dtype": "c64 (fp32)" if a.precision == "fp32" else
                      "c64 (fp32; forward x pass bf16 hi+lo x3 on tensor cores, fp32 accumulation)",
-            "precision": a.precision, "precision_check": precision_check,
+            "precision": a.precision, "precision_check": precision_check, "tensor_roofline": tensor_roofline,
             "cg_solves_per_s": value / (a.iters + 1), "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "apply_yardstick": yard, "kernels": per_kernel, "cpu_baseline": cpu,
             "clocks": clk, "setup_s": {"diagonals": t_diag, "diagonal_method": a.diag},
