@@ -29,6 +29,7 @@ struct hb_plan {
   int precision = HB_PRECISION_FP32;
   unsigned char* tc_ftab = nullptr;  // tensor-core pass A: DFT rows in operand layout
   int* tc_wait_error = nullptr;      // device address of g_tc_wait_error
+  int tc_stall_chunk = -1;           // fault injection for tests (hb_plan_inject_tc_stall)
 };
 
 namespace hb {
@@ -87,12 +88,27 @@ using PassLauncher = cudaError_t (*)(const PassArgs&, int, cudaStream_t);
 // hb_wait_status).
 __device__ int g_tc_wait_error;
 
+// Reads and clears g_tc_wait_error on the current device (synchronous; outside captures):
+// HB_ERR_CUDA with a message if a tensor-core pass gave up waiting.
+int tc_wait_check() {
+  int flag = 0;
+  const int zero = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&flag, g_tc_wait_error, sizeof(int));
+  if (e == cudaSuccess && flag) e = cudaMemcpyToSymbol(g_tc_wait_error, &zero, sizeof(int));
+  if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("tensor-core wait flag: ") + cudaGetErrorString(e));
+  if (flag)
+    return fail(HB_ERR_CUDA, "a tensor-core pass gave up waiting for its operands or contractions (about 1 s); "
+                             "its output is incomplete");
+  return HB_OK;
+}
+
 cudaError_t launch_a_tc(const hb_plan* p, const PassArgs& a, cudaStream_t st) {
   cudaError_t e = ensure_smem<expand_fwd_x_tc_kernel<128>>(tc::kSmemBytes);
   if (e != cudaSuccess) return e;
   dim3 grid(a.N0, a.nslots);
   LaunchScope ls(HB_KERNEL_EXPAND_FWD_X, st);
-  expand_fwd_x_tc_kernel<128><<<grid, tc::kThreadsAll, tc::kSmemBytes, st>>>(a, p->tc_ftab, p->tc_wait_error);
+  expand_fwd_x_tc_kernel<128><<<grid, tc::kThreadsAll, tc::kSmemBytes, st>>>(a, p->tc_ftab, p->tc_wait_error,
+                                                                             p->tc_stall_chunk);
   return cudaGetLastError();
 }
 
@@ -665,6 +681,8 @@ int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int it
     s0 += g;
   }
   HB_CUDA(cudaStreamSynchronize(st));
+  if (p->precision == HB_PRECISION_BF16X3)
+    if (int r = tc_wait_check()) return r;  // an incomplete x pass invalidates every solve
   bool notpd = false;
   for (int64_t i = 0; i < nsys; ++i) {
     if (status_host) status_host[i] = stat_all[i];
@@ -861,18 +879,18 @@ int hb_plan_set_precision(hb_plan* p, int precision) {
 
 int hb_plan_precision(const hb_plan* p) { return p ? p->precision : -1; }
 
+int hb_plan_inject_tc_stall(hb_plan* p, int chunk) {
+  if (int r = check_plan(p)) return r;
+  if (chunk < -1 || chunk >= p->N2 / tc::kKc)
+    return fail(HB_ERR_INVALID, "hb_plan_inject_tc_stall: chunk must be -1 or in [0, nx / 16)");
+  p->tc_stall_chunk = chunk;
+  return HB_OK;
+}
+
 int hb_wait_status(int device) {
   DeviceGuard dg(device);
   if (!dg.ok) return fail(HB_ERR_CUDA, "cannot select device " + std::to_string(device));
-  int flag = 0;
-  const int zero = 0;
-  cudaError_t e = cudaMemcpyFromSymbol(&flag, g_tc_wait_error, sizeof(int));
-  if (e == cudaSuccess && flag) e = cudaMemcpyToSymbol(g_tc_wait_error, &zero, sizeof(int));
-  if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("hb_wait_status: ") + cudaGetErrorString(e));
-  if (flag)
-    return fail(HB_ERR_CUDA, "a tensor-core pass gave up waiting for its operands or contractions (about 1 s); "
-                             "its output is incomplete");
-  return HB_OK;
+  return tc_wait_check();
 }
 
 int64_t hb_diag_packed_floats(const hb_plan* p) { return p ? 8LL * image_elems(p) : 0; }

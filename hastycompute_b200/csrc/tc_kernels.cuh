@@ -170,10 +170,11 @@ __device__ __forceinline__ void split_bf16x2(const float* v, uint32_t& hi, uint3
 
 // ftab: the forward DFT rows in operand layout, [chunk][re_hi, re_lo, im_hi,
 // im_lo][operand_offset] BF16 (kStageF bytes per chunk); wait_error: set to 1 when an
-// mbarrier wait gave up.
+// mbarrier wait gave up; stall_chunk: fault injection for tests, -1 in normal use (the
+// DFT-table copy of that chunk is not issued, so the wait for it runs out).
 template <int N2>
 __global__ void __launch_bounds__(tc::kThreadsAll, 1) expand_fwd_x_tc_kernel(PassArgs a, const unsigned char* ftab,
-                                                                             int* wait_error) {
+                                                                             int* wait_error, int stall_chunk) {
   using namespace tc;
   static_assert(N2 == 128, "tensor-core x pass: nx = 128");
   constexpr int M2 = 2 * N2, NCH = N2 / kKc;
@@ -215,27 +216,31 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 1) expand_fwd_x_tc_kernel(Pas
   if (warp == kThreads / 32) {
     if (lane == 0) {
       // ---- issuer: F table copies and the contractions ----
+      static_assert(NCH <= 32, "one bit per chunk");
+      uint32_t inflight = 0;  // chunks whose F copy was issued and not yet seen complete
       auto issue_f = [&](int c) {
+        if (c == stall_chunk) return;
         const int fs = c % kStagesF;
         mbar_expect_tx(smem_u32(&bar_full[fs]), kStageF);
         bulk_copy_g2s(sF + fs * kStageF, ftab + (size_t)c * kStageF, kStageF, smem_u32(&bar_full[fs]));
+        inflight |= 1u << c;
       };
-      int committed = -1, issued_f = -1, landed_f = -1;
+      int committed = -1;
       bool ok = true;
-      for (int c = 0; c < kFAhead && c < NCH; ++c) issue_f(issued_f = c);
+      for (int c = 0; c < kFAhead && c < NCH; ++c) issue_f(c);
 #pragma unroll 1
       for (int kc = 0; kc < NCH && ok; ++kc) {
         if (kc + kFAhead < NCH) {
           const int prev = kc + kFAhead - kStagesF;  // last user of that F slot
           if (prev >= 0 && !done_wait(prev)) { ok = false; break; }
-          issue_f(issued_f = kc + kFAhead);
+          issue_f(kc + kFAhead);
         }
         if (!mbar_wait(smem_u32(&bar_ready[kc % kStagesA]), (kc / kStagesA) & 1, abort) ||
             !mbar_wait(smem_u32(&bar_full[kc % kStagesF]), (kc / kStagesF) & 1, abort)) {
           ok = false;
           break;
         }
-        landed_f = kc;
+        inflight &= ~(1u << kc);
         tc_fence_after();
         const uint32_t sa = sbase + (kc % kStagesA) * kStageA, sf = sF + (kc % kStagesF) * kStageF;
         const uint64_t A0 = smem_desc(sa), A1 = smem_desc(sa + kArr), A2 = smem_desc(sa + 2 * kArr),
@@ -263,14 +268,18 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 1) expand_fwd_x_tc_kernel(Pas
       }
       if (!ok) abort_sh = 1;
       // before the shared memory is released: every commit's arrival and every copy in
-      // flight has landed (bounded waits that ignore the abort flag)
-      const long long t0 = clock64();
-      for (int c = committed; c >= 0 && c > committed - kDone; --c)
+      // flight has landed (waits bounded one by one, ignoring the abort flag)
+      for (int c = committed; c >= 0 && c > committed - kDone; --c) {
+        const long long t0 = clock64();
         while (!mbar_try_wait(smem_u32(&bar_done[c % kDone]), (c / kDone) & 1) && clock64() - t0 < kWaitCycles) {
         }
-      for (int c = landed_f + 1; c <= issued_f; ++c)
+      }
+      for (int c = 0; c < NCH; ++c) {
+        if (!(inflight & (1u << c))) continue;
+        const long long t0 = clock64();
         while (!mbar_try_wait(smem_u32(&bar_full[c % kStagesF]), (c / kStagesF) & 1) && clock64() - t0 < kWaitCycles) {
         }
+      }
     }
   } else {
     // ---- operand warps: task j (< 4) of a thread is row r = 32 j + 4 warp + lane / 8 and

@@ -84,8 +84,17 @@ int hb_plan_precision(const hb_plan* plan);
 
 /* Reads and clears the device's flag for a tensor-core pass that gave up waiting on one
  * of its mbarriers (after about one second): HB_ERR_CUDA with a message if it was set
- * (the output of that launch is incomplete), else HB_OK.  Synchronous. */
+ * (the output of that launch is incomplete), else HB_OK.  Synchronous.  hb_cg_run and
+ * hb_cg_run_systems check it themselves on plans set to HB_PRECISION_BF16X3; after the
+ * asynchronous calls (normal op, Toeplitz apply) the caller checks it. */
 int hb_wait_status(int device);
+
+/* Fault injection for tests of the path above (no counterpart in the reference): later
+ * tensor-core x passes of this plan omit the DFT-table copy of 16-sample chunk `chunk`
+ * (0 <= chunk < nx / 16), so each CTA's wait for it runs out after about one second and
+ * the CTA returns without writing its output; the device stays usable and hb_wait_status
+ * (or the CG's own check) reports it.  chunk = -1 turns it off (the default). */
+int hb_plan_inject_tc_stall(hb_plan* plan, int chunk);
 
 /* Number of floats of one packed diagonal (= 8 * nz * ny * nx). */
 int64_t hb_diag_packed_floats(const hb_plan* plan);

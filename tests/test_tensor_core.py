@@ -146,3 +146,35 @@ def test_cg_systems_that_converge_early_are_skipped(cuda, case):
     A = lambda v: O.sense_normal_toeplitz(v, sm, Ts[1])
     xo, _ = O.conjugate_gradient(A, bs[1], iters=6)
     assert O.rel_l2(_np(x[1]), xo) < TOL_ORACLE
+
+
+def test_a_wait_that_runs_out_is_reported_and_the_device_stays_usable(cuda):
+    """A wait made to run out (the plan omits one DFT-table copy, so nothing completes that
+    wait): each CTA gives up after about a second and returns without its output, the flag
+    reaches the host through hb_wait_status and through the CG's own check, and later calls
+    on the same device are correct."""
+    shape = (8, 128, 128)  # 8 CTAs per slot: about one second per stalled launch
+    rng = np.random.default_rng(51)
+    T = O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 100)), shape)
+    sm = synth.coil_maps(1, shape, seed=52)
+    x = synth.gaussian_image(shape, seed=53)
+    plan = ToeplitzPlan(shape, cuda, precision="bf16x3")
+    lib = plan.lib
+    packed = plan.pack_diagonal(_c64(T, cuda))
+    assert lib.hb_plan_inject_tc_stall(plan._h, 8) == capi.HB_ERR_INVALID
+    capi.check(lib.hb_plan_inject_tc_stall(plan._h, 3))
+    xi = _c64(x, cuda)
+    plan.apply_inplace(xi, packed)
+    with pytest.raises(capi.HastyError) as e:
+        plan.wait_status()
+    assert e.value.code == capi.HB_ERR_CUDA and "gave up waiting" in str(e.value)
+    plan.wait_status()  # read once, then cleared
+    b = _c64(O.sense_normal_toeplitz(x, sm, T), cuda)
+    with pytest.raises(capi.HastyError) as e:
+        plan.cg(torch.zeros_like(b), b, _c64(sm, cuda), packed, iters=1)
+    assert "gave up waiting" in str(e.value)
+    capi.check(lib.hb_plan_inject_tc_stall(plan._h, -1))
+    xi = _c64(x, cuda)
+    plan.apply_inplace(xi, packed)
+    plan.wait_status()
+    assert O.rel_l2(_np(xi), O.toeplitz_apply(x, T)) < TOL_ORACLE
