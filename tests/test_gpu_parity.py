@@ -136,6 +136,36 @@ def test_config1_size_normal_op(cuda):
     assert O.rel_l2(_np(out), ref) < TOL
 
 
+def test_config1_cg_matches_oracle(cuda):
+    """The CPU-runnable configuration end to end: 64^3, 8 coils, the 4096 x 128 kooshball,
+    b = A x_true + lambda x_true with lambda = 1e-3, 10-iteration CG; against the oracle's
+    FP64 CG on the same diagonal, and against the reference's own FP32 LibTorch CG
+    (opalgs.cpp:50-96 restated call for call).  CG amplifies rounding on this system: the
+    reference's FP32 CG lands 2.2e-3 from the FP64 one, this path's (FP64 scalars) 2.7e-4."""
+    shape = (64, 64, 64)
+    plan = ToeplitzPlan(shape, cuda)
+    coords = synth.kooshball(4096, 128)
+    packed, Tg = plan.build_diagonal(torch.from_numpy(coords), want_complex=True)
+    T = _np(Tg)
+    sm = synth.coil_maps(8, shape, seed=21)
+    xt = synth.gaussian_image(shape, seed=22).astype(np.complex128)
+    lam = 1e-3
+    b = O.sense_normal_toeplitz(xt, sm, T) + lam * xt
+    x = torch.zeros(shape, dtype=torch.complex64, device=cuda)
+    status, done = plan.cg(x, _c64(b, cuda), _c64(sm, cuda), packed, iters=10, lam=lam)
+    assert done == [10]
+    A = O.regularized(lambda v: O.sense_normal_toeplitz(v, sm, T), lam)
+    xo, _ = O.conjugate_gradient(A, b, iters=10)
+    from oracle import torch_ref as R
+
+    Ar = R.ToeplitzSenseNormalCPU(torch.from_numpy(T.astype(np.complex64)), torch.from_numpy(sm), lam=lam)
+    xr = torch.zeros((1,) + shape, dtype=torch.complex64)
+    R.conjugate_gradient(Ar, torch.from_numpy(b.astype(np.complex64)).reshape((1,) + shape), xr, iters=10)
+    e_gpu = O.rel_l2(_np(x), xo)
+    e_ref = O.rel_l2(xr.numpy()[0].astype(np.complex128), xo)
+    assert e_gpu < 1e-3 and e_gpu < e_ref
+
+
 def test_large_size_properties(cuda):
     """128^3 x 16 coils: Hermitian (<Ax,y> = <x,Ay>), linearity, bitwise determinism."""
     shape = (128, 128, 128)
