@@ -38,6 +38,8 @@ class NormalNufftToeplitz : public torch::CustomClassHolder {
     _op->apply_inplace(in, storage1, storage2);
   }
   at::Tensor get_diagonal() { return _op->get_diagonal(); }
+  // "fp32" (default) or "bf16x3" (forward x pass on the tensor cores, ny = nx = 128)
+  void set_precision(const std::string& name) { _op->plan()->set_precision(name); }
 
  private:
   std::unique_ptr<fft::CUDANormalNufftToeplitz> _op;
@@ -62,6 +64,8 @@ class SenseNormalToeplitz : public torch::CustomClassHolder {
     _op->apply(in, out, smaps, coils, imspace_storage, kspace_storage);
   }
   at::Tensor get_diagonal() { return _op->toeplitz()->get_diagonal(); }
+  // "fp32" (default) or "bf16x3" (forward x pass on the tensor cores, ny = nx = 128)
+  void set_precision(const std::string& name) { _op->toeplitz()->plan()->set_precision(name); }
 
  private:
   std::unique_ptr<mri::CUDASenseNormalToeplitz> _op;
@@ -136,12 +140,14 @@ TORCH_LIBRARY(HastyToeplitz, m) {
       .def("apply_add", &hasty::ffi::NormalNufftToeplitz::apply_add)
       .def("apply_addcmul", &hasty::ffi::NormalNufftToeplitz::apply_addcmul)
       .def("apply_inplace", &hasty::ffi::NormalNufftToeplitz::apply_inplace)
-      .def("get_diagonal", &hasty::ffi::NormalNufftToeplitz::get_diagonal);
+      .def("get_diagonal", &hasty::ffi::NormalNufftToeplitz::get_diagonal)
+      .def("set_precision", &hasty::ffi::NormalNufftToeplitz::set_precision);
 
   m.class_<hasty::ffi::SenseNormalToeplitz>("SenseNormalToeplitz")
       .def(torch::init<const std::optional<at::Tensor>&, const std::vector<int64_t>&, const std::optional<at::Tensor>&>())
       .def("apply", &hasty::ffi::SenseNormalToeplitz::apply)
-      .def("get_diagonal", &hasty::ffi::SenseNormalToeplitz::get_diagonal);
+      .def("get_diagonal", &hasty::ffi::SenseNormalToeplitz::get_diagonal)
+      .def("set_precision", &hasty::ffi::SenseNormalToeplitz::set_precision);
 
   m.class_<hasty::ffi::BatchedSenseNormalToeplitz>("BatchedSenseNormalToeplitz")
       .def(torch::init<const at::Tensor&, const at::Tensor&, const std::optional<std::vector<int64_t>>&>())

@@ -33,6 +33,11 @@ class NormalNufftToeplitz:
     def get_diagonal(self):
         return self._op.get_diagonal()
 
+    def set_precision(self, precision):
+        """"fp32" (default) or "bf16x3": the forward x pass as a tensor-core contraction with
+        BF16 hi + lo operands and FP32 accumulation (ny = nx = 128)."""
+        self._op.set_precision(precision)
+
 
 class SenseNormalToeplitz:
     """Toeplitz twin of hastypy.ffi.hasty_sense.SenseNormal (same apply signature)."""
@@ -45,6 +50,11 @@ class SenseNormalToeplitz:
 
     def get_diagonal(self):
         return self._senseop.get_diagonal()
+
+    def set_precision(self, precision):
+        """"fp32" (default) or "bf16x3": the forward x pass as a tensor-core contraction with
+        BF16 hi + lo operands and FP32 accumulation (ny = nx = 128)."""
+        self._senseop.set_precision(precision)
 
 
 class BatchedSenseNormalToeplitz:

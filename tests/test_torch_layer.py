@@ -102,7 +102,22 @@ def test_batched_sense_reduced_precision_through_the_torchscript_class(ffi, cuda
     x = torch.from_numpy(synth.gaussian_image((1, 1) + shape, seed=8))
     out = torch.empty_like(x)
     op.apply(x, out, [[0, 1]])
-    assert O.rel_l2(out[0, 0].numpy(), O.sense_normal_toeplitz(x[0, 0].numpy(), sm, T, [0, 1])) < 1e-4
+    ref = O.sense_normal_toeplitz(x[0, 0].numpy(), sm, T, [0, 1])
+    assert O.rel_l2(out[0, 0].numpy(), ref) < 1e-4
+    # the single-operator classes take the same switch
+    sop = ffi.SenseNormalToeplitz(None, [1] + list(shape), torch.from_numpy(T[None].astype(np.complex64)).to(cuda))
+    sop.set_precision("bf16x3")
+    xs = x[0].to(cuda)
+    outs = torch.empty_like(xs)
+    sop.apply(xs, outs, torch.from_numpy(sm).to(cuda), [0, 1])
+    assert O.rel_l2(outs[0].cpu().numpy(), ref) < 1e-4
+    top = ffi.NormalNufftToeplitz(None, [1] + list(shape), torch.from_numpy(T[None].astype(np.complex64)).to(cuda))
+    top.set_precision("bf16x3")
+    xi = xs.clone()
+    s1 = torch.empty((1,) + tuple(2 * n for n in shape), dtype=torch.complex64, device=cuda)
+    s2 = torch.empty_like(s1)
+    top.apply_inplace(xi, s1, s2)
+    assert O.rel_l2(xi[0].cpu().numpy(), O.toeplitz_apply(x[0, 0].numpy(), T)) < 1e-4
 
 
 def test_legacy_batched_binding_in_place(ffi, cuda):
