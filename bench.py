@@ -511,7 +511,12 @@ def main():
     # in proportion to its slots, so a full launch is that figure x slots
     traffic_per_slot = {"expand_fwd_x": 766.4e6 / 16, "plane_yz": 1084.0e6 / 16, "inv_x_combine": 839.6e6 / 16}
     traffic = traffic_per_slot[dom] * C * nsys if a.n == 128 else None
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+    sched = plan.plane_schedule()
+    kernel_name = {"expand_fwd_x": f"expand_fwd_x_kernel<{a.n},16>",
+                   "inv_x_combine": f"inv_x_combine_kernel<{a.n},16>",
+                   "plane_yz": (f"plane_mod_kernel ({sched})" if sched.startswith("mod")
+                                else f"plane_yz_kernel ({sched})")}[dom]
+    roofline = {"bound": "hbm", "kernel": kernel_name, "profile_kind": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_src, "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_read+write of one 16-slot launch, scaled by slots"
                 if traffic is not None else None,

@@ -77,6 +77,7 @@ SIGNATURES = {
     "hb_toeplitz_apply_noalloc": (c_int, [c_i64, c_i64, c_i64, c_void_p, c_void_p, c_i64, c_i64, c_void_p, c_int,
                                           c_void_p, c_void_p]),
     "hb_autotune_workspace_bytes": (c_size, [c_void_p, c_i64]),
+    "hb_plan_plane_schedule": (ctypes.c_char_p, [c_void_p]),
     "hb_plan_autotune": (c_int, [c_void_p, c_i64, c_void_p, c_size, c_void_p, ctypes.POINTER(c_int),
                                  ctypes.POINTER(c_double)]),
     "hb_nufft_create": (c_int, [ctypes.POINTER(c_void_p), c_i64, c_i64, c_i64, c_void_p, c_i64, c_double, c_int,

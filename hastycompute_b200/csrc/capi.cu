@@ -777,6 +777,8 @@ void fill_tables(float2* h, int N0, int N1, int N2) {
 // ------------------------------------------------ allocation-free Toeplitz apply ----
 // The spill and the twiddle tables of hb_toeplitz_apply_noalloc live in these arrays;
 // host code reaches them only through cudaGetSymbolAddress (per device).
+// Sized for table_offsets(160, 160, 160).total, the largest supported axes; each call
+// checks its own size against it.
 constexpr int kNoAllocMaxTables = 2 * 160 + 160 + 2 * 160 + 160 + 80 + 40 + 2 * 160;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[HB_NOALLOC_SCRATCH_BYTES];
 static __device__ __align__(256) float2 g_noalloc_tables[kNoAllocMaxTables];
@@ -1075,6 +1077,12 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
                                       " bytes of scratch, more than the built-in " +
                                       std::to_string((unsigned long long)HB_NOALLOC_SCRATCH_BYTES) +
                                       " (use hb_toeplitz_apply with a caller workspace)");
+  // the built-in twiddle-table array holds the tables of axes up to 160; a size whose
+  // tables would not fit is refused before anything is written
+  if (table_offsets((int)nz, (int)ny, (int)nx).total > kNoAllocMaxTables)
+    return fail(HB_ERR_UNSUPPORTED, "hb_toeplitz_apply_noalloc: twiddle tables of " + std::to_string(nz) + "x" +
+                                        std::to_string(ny) + "x" + std::to_string(nx) + " exceed the built-in " +
+                                        std::to_string(kNoAllocMaxTables) + " entries");
   int dev = 0;
   HB_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(HB_ERR_INVALID, "hb_toeplitz_apply_noalloc: device index");
@@ -1128,6 +1136,14 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
   a.out_ldy = out_ldy;
   a.accumulate = accumulate ? 1 : 0;
   return run_normal(&p, a, st);
+}
+
+const char* hb_plan_plane_schedule(const hb_plan* p) {
+  if (!p) return "";
+  int n = 0;
+  const PlaneVariant* v = plane_variants(p->N0, p->N1, &n);
+  if (!v) return "plane_yz:q1";
+  return v[plane_variant_index(n, p->plane_variant)].name;
 }
 
 size_t hb_autotune_workspace_bytes(const hb_plan* p, int64_t nslots) {

@@ -121,6 +121,10 @@ class ToeplitzPlan:
             self._ws = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
         return self._ws
 
+    def plane_schedule(self):
+        """Name of the plane-pass schedule the next call launches (``hb_plan_plane_schedule``)."""
+        return self.lib.hb_plan_plane_schedule(self._h).decode()
+
     def autotune(self, nslots=16):
         """Times the plane-pass schedules on nslots (system, coil) slots and keeps the
         fastest for this plan.  Returns (schedule index, ms per launch)."""

@@ -202,6 +202,12 @@ int hb_cg_run(const hb_plan* plan, int64_t nsys, void* x, const void* b, const v
  * Synchronises `stream`.  chosen / best_ms (nullable) receive the schedule index and its
  * time per launch.  The environment variable HB_PLANE_VARIANT, when set, overrides. */
 size_t hb_autotune_workspace_bytes(const hb_plan* plan, int64_t nslots);
+/* Name of the plane-pass schedule the plan's next call launches ("mod4t256": the ky-mod-4
+ * split plane_mod_kernel, 4-CTA clusters of 256 threads; "q2t128": the parity split
+ * plane_yz_kernel, 2x2-CTA clusters of 128 threads; ...), after HB_PLANE_VARIANT and
+ * hb_plan_autotune.  A static string owned by the library.  No counterpart in the
+ * reference (cuFFT chooses its own plans, nufft.cpp:1184-1186). */
+const char* hb_plan_plane_schedule(const hb_plan* plan);
 int hb_plan_autotune(hb_plan* plan, int64_t nslots, void* workspace, size_t workspace_bytes,
                      void* stream, int* chosen, double* best_ms);
 
@@ -219,8 +225,16 @@ int hb_plan_autotune(hb_plan* plan, int64_t nslots, void* workspace, size_t work
  * Limits and behaviour:
  *  - 16 * nz * ny * nx must not exceed HB_NOALLOC_SCRATCH_BYTES (16 MiB: up to 2^20
  *    voxels, e.g. 128 x 128 x 64); larger sizes return HB_ERR_WORKSPACE with a message.
+ *  - Sizes whose twiddle tables exceed the built-in table array return
+ *    HB_ERR_UNSUPPORTED (every size hb_size_supported accepts fits).
  *  - Works on the calling thread's current device.  The first call on a device looks up
  *    the arrays' device addresses; make that first call before any stream capture.
+ *  - Every call copies its descriptor block (and, when the size differs from the
+ *    previous call's on this device, the twiddle tables) from host memory with
+ *    cudaMemcpyAsync on `stream` and then waits for `stream` with
+ *    cudaStreamSynchronize, so the call returns only after the work queued on `stream`
+ *    before it has finished; the three passes themselves are then queued on `stream`
+ *    without waiting.  hb_toeplitz_apply does the same through its table upload.
  *  - All calls share the arrays, which keep the last call's contents (nothing in them
  *    needs to start at zero).  Calls that overlap on the GPU (several streams or
  *    threads) race on the shared scratch: serialise them.

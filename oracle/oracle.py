@@ -106,6 +106,37 @@ def sense_normal_toeplitz(x, smaps, T, coils=None):
     return out
 
 
+# ---- the same two restatements on complex128 torch tensors ----
+# At the benchmark's size (128^3 images, 256^3 grid, 16 coils) numpy's FFTs take minutes per
+# CG solve.  These restate nufft.cpp:1163-1197 and sense.ixx:500-578 line for line with
+# torch.fft in complex128 (FP64), on whichever device the tensors live on; the CG below
+# accepts them as well.  tests/test_oracle.py pins them to the numpy versions above.
+
+def toeplitz_apply_t(x, T):
+    """``toeplitz_apply`` for complex128 torch tensors: crop(ifftn(T * fftn(x, s=M)))."""
+    import torch
+
+    N = tuple(x.shape)
+    F = torch.fft.fftn(x.to(torch.complex128), s=tuple(T.shape), dim=(0, 1, 2))
+    F.mul_(T)
+    y = torch.fft.ifftn(F, dim=(0, 1, 2))
+    return y[: N[0], : N[1], : N[2]]
+
+
+def sense_normal_toeplitz_t(x, smaps, T, coils=None):
+    """``sense_normal_toeplitz`` for complex128 torch tensors (x [N], smaps [C, N], T [M])."""
+    import torch
+
+    x = x.to(torch.complex128)
+    if coils is None:
+        coils = range(smaps.shape[0])
+    out = torch.zeros_like(x)
+    for c in coils:
+        s = smaps[c].to(torch.complex128)
+        out += s.conj() * toeplitz_apply_t(x * s, T)
+    return out
+
+
 def explicit_normal(x, coords, weights=None):
     """Explicit NUFFT normal op on the N grid (type-2 isign -1, type-1 isign +1, each
     scaled 1/sqrt(prod(N)); ``nufft.cpp:104-123,785-920``), as a dense direct NUDFT."""
@@ -245,8 +276,16 @@ def admm_llr(A_of_system, b0, x0, rho, svt, admm_iters, cg_iters):
     return x, z
 
 
+def _is_torch(a):
+    return type(a).__module__.split(".")[0] == "torch"
+
+
 def vdot(a, b):
-    """``vdot`` (``lib/op/vec.cpp:624-637``): sum(conj(a) * b)."""
+    """``vdot`` (``lib/op/vec.cpp:624-637``): sum(conj(a) * b), in FP64."""
+    if _is_torch(a):
+        import torch
+
+        return complex(torch.vdot(a.flatten(), b.flatten()).item())
     return np.vdot(np.asarray(a).ravel(), np.asarray(b).ravel())
 
 
@@ -257,15 +296,22 @@ class NotPositiveDefinite(RuntimeError):
 def conjugate_gradient(A, b, x0=None, iters=30, tol=0.0, P=None):
     """``ConjugateGradient::run`` (``lib/op/opalgs.cpp:50-96``), float64.
 
-    Returns (x, n_done) where n_done counts the iterations that updated x.
+    Returns (x, n_done) where n_done counts the iterations that updated x.  b (and x0) are
+    numpy arrays or torch tensors; either way the vectors are complex128.
     """
-    b = np.asarray(b, np.complex128)
-    x = np.zeros_like(b) if x0 is None else np.array(x0, np.complex128)
+    if _is_torch(b):
+        import torch
+
+        b = b.to(torch.complex128)
+        x = torch.zeros_like(b) if x0 is None else x0.to(torch.complex128).clone()
+    else:
+        b = np.asarray(b, np.complex128)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, np.complex128)
     if iters < 1:
         return x, 0
     r = b - A(x)
     z = P(r) if P is not None else r
-    p = z.copy()
+    p = z.clone() if _is_torch(z) else z.copy()
     rzold = vdot(r, z).real
     resid = np.sqrt(rzold)
     done = 0
@@ -294,6 +340,13 @@ def regularized(A, lam):
 
 
 def rel_l2(a, b):
+    if _is_torch(a) or _is_torch(b):
+        import torch
+
+        dev = a.device if _is_torch(a) else b.device
+        a = (a if _is_torch(a) else torch.from_numpy(np.asarray(a))).to(dev, torch.complex128)
+        b = (b if _is_torch(b) else torch.from_numpy(np.asarray(b))).to(dev, torch.complex128)
+        return float(torch.linalg.vector_norm(a - b) / max(float(torch.linalg.vector_norm(b)), 1e-300))
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))

@@ -29,9 +29,13 @@ class ToeplitzSenseNormalCPU:
         self.lam = float(lam)
         self.N = tuple(smaps.shape[-3:])
         self.M = tuple(self.T.shape[-3:])
-        self.s1 = torch.empty((1,) + self.M, dtype=torch.complex64)
-        self.s2 = torch.empty((1,) + self.M, dtype=torch.complex64)
-        self.imstore = torch.empty((1,) + self.N, dtype=torch.complex64)
+        # storage on the diagonal's device: on a CUDA device the same calls are the
+        # reference's own GPU path (cuFFT through at::fft_fftn_out, ATen elementwise kernels)
+        dev = self.T.device
+        self.smaps = self.smaps.to(dev)
+        self.s1 = torch.empty((1,) + self.M, dtype=torch.complex64, device=dev)
+        self.s2 = torch.empty((1,) + self.M, dtype=torch.complex64, device=dev)
+        self.imstore = torch.empty((1,) + self.N, dtype=torch.complex64, device=dev)
 
     def apply_addcmul(self, inp, add_to, mul):
         torch.fft.fftn(inp, s=self.M, dim=(1, 2, 3), out=self.s1)
