@@ -530,11 +530,18 @@ plane_mod_kernel(PassArgs a) {
   const float* T = a.sys_diag[sys] + (((long long)kx * 2 + (q & 1)) * N1) * M0;
 
   // stage 1: rows.  Lane t of a row team loads y' + L*m for y' = t + SR*e, folds with
-  // the K-th roots of unity, twiddles once by w_M1^(y'*q), then an L-point FFT.
+  // the K-th roots of unity, twiddles once by w_M1^(y'*q), then an L-point FFT.  Lane t
+  // uses the same row-FFT twiddles (tw_r[k1*SR + t]) and fold twiddles w_M1^(y'*q) for
+  // every row: they are read from shared memory once, into registers (stage 3 likewise).
   {
     const int team = threadIdx.x / SR, t = threadIdx.x % SR;
     const int tr = row_of_team<SR, C::NTEAMS_R, N0>(team);
     float2* buf = xbuf + team * C::TBUF_R;
+    float2 twr[ER];
+    load_lane_twiddles<L>(twr, tw_r, t);
+    float2 cw[ER];
+#pragma unroll
+    for (int e = 0; e < ER; ++e) cw[e] = circ[(din_index<L>(t, e) * q) % M1];
     float2 nv[NM][ER];  // the next row's values, loaded while the current one is transformed
     {
       const float2* row = g + (long long)(tr < N0 ? tr : 0) * RS;
@@ -552,7 +559,7 @@ plane_mod_kernel(PassArgs a) {
         float2 acc = nv[0][e];
 #pragma unroll
         for (int m = 1; m < NM; ++m) acc = cadd(acc, rootK<K, -1>(nv[m][e], m * q));
-        v[e] = q == 0 ? acc : cmul(acc, circ[(din_index<L>(t, e) * q) % M1]);
+        v[e] = q == 0 ? acc : cmul(acc, cw[e]);
       }
       if (it + 1 < C::LPT) {
         const int zn = z + C::NTEAMS_R;
@@ -562,7 +569,7 @@ plane_mod_kernel(PassArgs a) {
 #pragma unroll
           for (int e = 0; e < ER; ++e) nv[m][e] = row[din_index<L>(t, e) + L * m];
       }
-      team_fft_din_to_dout<L, -1, false>(v, t, buf, tw_r);
+      team_fft_din_to_dout_r<L, -1, false>(v, t, buf, twr);
       if (z < N0) {
 #pragma unroll
         for (int r = 0; r < ER; ++r) P[z * LDP + dout_index<L>(t, r)] = v[r];
@@ -622,6 +629,8 @@ plane_mod_kernel(PassArgs a) {
     const int team = threadIdx.x / SR, t = threadIdx.x % SR;
     const int tr = row_of_team<SR, C::NTEAMS_R, N0>(team);
     float2* buf = xbuf + team * C::TBUF_R;
+    float2 twr[ER];
+    load_lane_twiddles<L>(twr, tw_r, t);
 #pragma unroll 1
     for (int it = 0; it < C::LPT; ++it) {
       const int z = tr + it * C::NTEAMS_R;
@@ -629,7 +638,7 @@ plane_mod_kernel(PassArgs a) {
       float2 v[ER];
 #pragma unroll
       for (int r = 0; r < ER; ++r) v[r] = P[zc * LDP + dout_index<L>(t, r)];
-      team_fft_dout_to_din<L, 1, false>(v, t, buf, tw_r);
+      team_fft_dout_to_din_r<L, 1, false>(v, t, buf, twr);
       if (z < N0) {
 #pragma unroll
         for (int e = 0; e < ER; ++e) P[z * LDP + din_index<L>(t, e)] = v[e];
@@ -645,12 +654,17 @@ plane_mod_kernel(PassArgs a) {
 #pragma unroll
     for (int qq = 0; qq < K; ++qq) R[qq] = cluster.map_shared_rank(P, qq);
     constexpr int ROWS = N0 / K;
+    static_assert(C::THREADS % L == 0, "a thread keeps its y through the stage-4 loop");
+    const int y = threadIdx.x % L;  // the same for every item of this thread
+    float2 cy[K];                   // w_M1^(y*qq), from registers
+#pragma unroll
+    for (int qq = 1; qq < K; ++qq) cy[qq] = circ[(y * qq) % M1];
     for (int i = threadIdx.x; i < ROWS * L; i += C::THREADS) {
-      const int z = q * ROWS + i / L, y = i % L;
+      const int z = q * ROWS + i / L;
       float2 u[K];
       u[0] = R[0][z * LDP + y];
 #pragma unroll
-      for (int qq = 1; qq < K; ++qq) u[qq] = cmulc(R[qq][z * LDP + y], circ[(y * qq) % M1]);
+      for (int qq = 1; qq < K; ++qq) u[qq] = cmulc(R[qq][z * LDP + y], cy[qq]);
       Dft<K, 1>::run(u);
 #pragma unroll
       for (int m = 0; m < NM; ++m) g[(long long)z * RS + y + L * m] = u[m];

@@ -405,3 +405,17 @@ def test_cg_host_buffers_match_device_cg(cuda):
     assert it == [6] * 5
     assert torch.equal(out, xd.cpu())
     assert float(xh.abs().max()) == 0.0  # the initial guess is read, not overwritten
+
+
+def test_bench_unpacks_the_packed_diagonal(cuda):
+    """bench.py's accuracy report rebuilds Re(T) from the packed diagonal the plans read;
+    it must equal Re(T) of the reference-layout diagonal that was packed."""
+    import bench
+
+    shape = (8, 16, 32)
+    coords, x, sm, T = _case(shape, 1, 500, 41)
+    plan = ToeplitzPlan(shape, cuda)
+    packed = plan.pack_diagonal(_c64(T, cuda)).unsqueeze(0)
+    got = bench.unpack_diagonal(plan, packed)(0)
+    want = torch.from_numpy(T.real.astype(np.float32).astype(np.float64)).to(cuda)
+    assert torch.allclose(got.real, want, rtol=1e-6, atol=0) and float(got.imag.abs().max()) == 0.0
