@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--jobs", type=int, default=64, help="uneven/serve: jobs in the mix (serve: pool size)")
     ap.add_argument("--max-frames", type=int, default=20)
     ap.add_argument("--rates", default="1,2,4", help="serve: arrival rates (jobs/s)")
+    ap.add_argument("--engine", default="batch", choices=["batch", "groups"],
+                    help="uneven/serve: running batches with iteration-boundary admission (batch), or fixed "
+                         "groups / per-job streams (groups)")
     ap.add_argument("--duration", type=float, default=30.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", default="both", choices=["both", "fp32", "bf16x3"],
@@ -282,10 +285,43 @@ def uneven_once(a, dev):
     sysl = {k: systems_of(k) for k in classes}
     streams = {k: torch.cuda.Stream(dev) for k in classes}
 
+    batches = {}
+    if a.engine == "batch":
+        # one running batch per size class, capacity from the same workspace share
+        for k in classes:
+            nv = k[0] * k[1] * k[2]
+            slots = max(32, int(ws_cap // (16 * nv + 24 * nv // 8 + 1)))
+            nsysk = max(1, slots // 4)
+            while slots > 32 and plans[k].lib.hb_cg_batch_workspace_bytes(plans[k]._h, nsysk, slots) > ws_cap:
+                slots = int(slots * 0.9)
+                nsysk = max(1, slots // 4)
+            batches[k] = plans[k].cg_batch(nsysk, slots)
+
+    def run_batch(k):
+        """Every system of size class k through its running batch: systems join as members
+        leave (at iteration boundaries), one launch sequence per iteration."""
+        bt = batches[k]
+        queue = list(sysl[k])
+        pos, left = 0, len(queue)
+        while left:
+            while pos < len(queue):
+                try:
+                    bt.add(queue[pos], a.iters)
+                except capi.HastyError as e:
+                    if e.code != capi.HB_ERR_WORKSPACE:
+                        raise
+                    break
+                pos += 1
+            bt.step(streams[k])
+            left -= len(bt.retire())
+
     def solve(k, errs):
         try:
             with torch.cuda.stream(streams[k]):
-                plans[k].cg_systems(sysl[k], iters=a.iters, graph=True, workspace_bytes=ws_cap)
+                if a.engine == "batch":
+                    run_batch(k)
+                else:
+                    plans[k].cg_systems(sysl[k], iters=a.iters, graph=True, workspace_bytes=ws_cap)
         except Exception as e:  # noqa: BLE001
             errs.append(e)
 
@@ -325,8 +361,13 @@ def uneven_once(a, dev):
         "ms_per_step": ms / a.steps, "higher_is_better": True, "data": "synthetic (seeded)", "precision": a.precision,
         "dtype": "c64 (fp32)" if a.precision == "fp32" else "c64 (fp32; 128^3 jobs: forward x pass bf16 hi+lo x3)",
         "config": {"workload": f"{a.jobs} jobs, sizes {MIX_SHAPES}, coils {MIX_COILS}, 1-{a.max_frames} frames, "
-                               f"1000-4000 spokes x {a.samples}, {a.iters}-iteration CG, one launch sequence per size "
-                               f"class on its own stream, iterations replayed as CUDA graphs",
+                               f"1000-4000 spokes x {a.samples}, {a.iters}-iteration CG, "
+                               + ("one running batch per size class (systems join at iteration boundaries as "
+                                  "members finish; one launch sequence per iteration), each on its own stream"
+                                  if a.engine == "batch" else
+                                  "one launch sequence per size class on its own stream, groups of systems that "
+                                  "fit the workspace, iterations replayed as CUDA graphs"),
+                   "engine": a.engine,
                    "systems": nsys, "jobs_per_size": {str(k): len(v) for k, v in classes.items()},
                    "autotuned_plane_schedule": tuned},
         "gpu_launches": capi.launch_count() - launches0, "clocks": clk, "setup_s": setup,
@@ -349,7 +390,10 @@ def run_serve(a, dev):
                      "c64 (fp32; 128^3 jobs: forward x pass bf16 hi+lo x3)",
             "config": {"workload": f"Poisson arrivals, job pool of {a.jobs} as in the uneven mix with 1-{a.max_frames} "
                                    f"frames, {a.duration:.0f} s per rate, {a.iters}-iteration CG, admission by HBM "
-                                   f"footprint, per-job streams (up to 4 concurrent)"},
+                                   f"footprint, "
+                                   + ("continuous batching: one running batch per image size, systems join at "
+                                      "iteration boundaries" if a.engine == "batch" else
+                                      "per-job streams (up to 4 concurrent)")},
             "per_rate": head}
     if len(precs) == 2:
         line["reduced"] = {"precision": "bf16x3", "value": max(r["p99_s"] for r in per["bf16x3"]),
@@ -371,7 +415,8 @@ def serve_rates(a, dev):
     results = []
     for rate in [float(r) for r in a.rates.split(",")]:
         server = ReconServer(dev, hbm_budget_bytes=int(torch.cuda.mem_get_info(dev)[0] * 0.6), max_active=4,
-                             precision=a.precision)
+                             precision=a.precision, mode="batching" if a.engine == "batch" else "streams",
+                             sizes=sorted({j["shape"] for j in pool}))
         # warm one job through the path
         j0 = pool[0]
         server.submit(ReconJob(j0["shape"], j0["smaps"], j0["packed"], [0] * j0["frames"], j0["b"],
@@ -615,7 +660,9 @@ def main():
             served[prec] = serve_rates(sa, dev)[0]
         served["config"] = (f"Poisson arrivals at {a.serve_rate} jobs/s for {a.serve_seconds:.0f} s per plan, pool of "
                             f"{a.serve_jobs} jobs drawn as in the uneven mix with 1-{a.serve_max_frames} frames, "
-                            f"{a.iters}-iteration CG, admission by HBM footprint, up to 4 concurrent jobs")
+                            f"{a.iters}-iteration CG, admission by HBM footprint, "
+                            + ("continuous batching (one running batch per image size)" if a.engine == "batch"
+                               else "up to 4 concurrent jobs on their own streams"))
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -700,17 +747,34 @@ def accuracy_report(a, plan, res, sm, packed, xtrue, b, diag_index, dev):
     return out
 
 
+TEAM_SHAPE = {8: (4, 2), 16: (4, 4), 32: (8, 4), 64: (8, 8), 128: (16, 8), 256: (16, 16), 96: (24, 4),
+              160: (40, 4), 192: (24, 8), 320: (40, 8), 512: (32, 16)}
+
+
+def column_kz(m0):
+    """kz held at each position p = t*E + r of a packed z column: the z transform's output
+    index (t + S*(r//S)) + E*(r%S) of lane t, register r (E, S: the team shape of m0)."""
+    E, S = TEAM_SHAPE[m0]
+    p = np.arange(m0)
+    t, r = p // E, p % E
+    return (t + S * (r // S)) + E * (r % S)
+
+
 def unpack_diagonal(plan, packed):
     """Reference-layout Re(T) (complex128, [2nz, 2ny, 2nx]) of frame f from the packed
-    diagonals the plans read: packed[f] holds Re(T)/prod(2N) as [kx][h][ky'][kz] with
-    ky = 2ky' + h (the layout hb_diag_pack writes).  Im(T) never reaches the cropped
-    output, so Re(T) gives the reference operator exactly."""
+    diagonals the plans read: packed[f] holds Re(T)/prod(2N) as [kx][h][ky'][p] with
+    ky = 2ky' + h and each z column in lane order (position p holds kz = column_kz(p);
+    the layout hb_diag_pack writes).  Im(T) never reaches the cropped output, so Re(T)
+    gives the reference operator exactly."""
     n0, n1, n2 = plan.shape
     m0, m1, m2 = 2 * n0, 2 * n1, 2 * n2
+    kz_of = torch.from_numpy(column_kz(m0))
 
     def get(f):
         p = packed[f].to(torch.float64).reshape(m2, 2, n1, m0) * float(m0 * m1 * m2)
-        t = p.permute(3, 2, 1, 0).reshape(m0, m1, m2)  # [kz][ky' * 2 + h][kx]
+        col = torch.empty_like(p)
+        col[..., kz_of.to(p.device)] = p  # back to natural kz order
+        t = col.permute(3, 2, 1, 0).reshape(m0, m1, m2)  # [kz][ky' * 2 + h][kx]
         return t.to(torch.complex128)
     return get
 

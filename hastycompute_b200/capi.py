@@ -78,6 +78,12 @@ SIGNATURES = {
                                           c_void_p, c_void_p]),
     "hb_autotune_workspace_bytes": (c_size, [c_void_p, c_i64]),
     "hb_plan_plane_schedule": (ctypes.c_char_p, [c_void_p]),
+    "hb_cg_batch_workspace_bytes": (c_size, [c_void_p, c_i64, c_i64]),
+    "hb_cg_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_void_p, c_i64, c_i64, c_void_p, c_size]),
+    "hb_cg_batch_destroy": (c_int, [c_void_p]),
+    "hb_cg_batch_add": (c_int, [c_void_p, c_void_p, c_int, c_double, ctypes.POINTER(c_i64)]),
+    "hb_cg_batch_step": (c_int, [c_void_p, c_void_p, ctypes.POINTER(c_i64)]),
+    "hb_cg_batch_retire": (c_int, [c_void_p, P_i64, P_i32, P_i32, c_i64, ctypes.POINTER(c_i64)]),
     "hb_plan_autotune": (c_int, [c_void_p, c_i64, c_void_p, c_size, c_void_p, ctypes.POINTER(c_int),
                                  ctypes.POINTER(c_double)]),
     "hb_nufft_create": (c_int, [ctypes.POINTER(c_void_p), c_i64, c_i64, c_i64, c_void_p, c_i64, c_double, c_int,

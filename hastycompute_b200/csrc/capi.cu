@@ -97,7 +97,7 @@ int tc_wait_check() {
   if (e == cudaSuccess && flag) e = cudaMemcpyToSymbol(g_tc_wait_error, &zero, sizeof(int));
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("tensor-core wait flag: ") + cudaGetErrorString(e));
   if (flag)
-    return fail(HB_ERR_CUDA, "a tensor-core pass gave up waiting for its operands or contractions (about 1 s); "
+    return fail(HB_ERR_CUDA, "a pass gave up waiting for a bulk copy, its operands or its contractions (about 1 s); "
                              "its output is incomplete");
   return HB_OK;
 }
@@ -476,8 +476,15 @@ PassArgs group_pass_args(const hb_plan* p, const GroupWs& w, int64_t g, int64_t 
   a.out_ldy = p->N2;
   a.accumulate = 0;
   a.dot_partials = nullptr;
+  a.wait_error = p->tc_wait_error;
   return a;
 }
+
+// The plane pass reads each packed z column with 16-byte vector loads.
+bool diag_aligned(const float* d) { return ((uintptr_t)d & 15u) == 0; }
+// Passes A and C move spill tiles with bulk copies, which need 16-byte aligned addresses;
+// the workspace is carved at 256-byte offsets from its start.
+bool ws_aligned(const void* w) { return ((uintptr_t)w & 15u) == 0; }
 
 int validate_systems(const hb_plan* p, int64_t nsys, const hb_system* sys, bool cg) {
   if (nsys < 1 || !sys) return fail(HB_ERR_INVALID, "no systems");
@@ -485,6 +492,8 @@ int validate_systems(const hb_plan* p, int64_t nsys, const hb_system* sys, bool 
     const hb_system& q = sys[i];
     if (!q.x || !q.smaps || !q.packed_diag || (q.ncoil > 0 && !q.coils))
       return fail(HB_ERR_INVALID, "system " + std::to_string(i) + ": NULL pointer");
+    if (!diag_aligned(q.packed_diag))
+      return fail(HB_ERR_INVALID, "system " + std::to_string(i) + ": packed diagonal not 16-byte aligned");
     if (cg ? !q.b : !q.out) return fail(HB_ERR_INVALID, "system " + std::to_string(i) + ": NULL pointer");
     if (q.ncoil < 1 || q.ncoil > 65535) return fail(HB_ERR_INVALID, "system " + std::to_string(i) + ": ncoil");
     for (int64_t c = 0; c < q.ncoil; ++c)
@@ -593,6 +602,7 @@ int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int it
     const int64_t g = next_group(p, sys, s0, nsys, iters, true, ws_bytes, &slots);
     if (!ws || group_bytes(p, g, slots, iters, true) > ws_bytes)
       return fail(HB_ERR_WORKSPACE, "hb_cg_run: workspace too small for one system");
+    if (!ws_aligned(ws)) return fail(HB_ERR_INVALID, "hb_cg_run: workspace not 16-byte aligned");
     Arena ar(ws);
     GroupWs w = carve_group(ar, p, g, slots, iters, true);
     if (int r = upload_tables(p, w, sys, s0, g, true, st)) return r;
@@ -681,8 +691,9 @@ int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int it
     s0 += g;
   }
   HB_CUDA(cudaStreamSynchronize(st));
-  if (p->precision == HB_PRECISION_BF16X3)
-    if (int r = tc_wait_check()) return r;  // an incomplete x pass invalidates every solve
+  // a pass that gave up waiting for a copy (or, on tensor-core plans, a contraction) left
+  // its output incomplete, which invalidates every solve
+  if (int r = tc_wait_check()) return r;
   bool notpd = false;
   for (int64_t i = 0; i < nsys; ++i) {
     if (status_host) status_host[i] = stat_all[i];
@@ -693,6 +704,84 @@ int cg_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, int it
   return HB_OK;
 }
 
+// ------------------------------------------------------- running batch of CG solves ----
+// Layout of the per-member arrays that follow the pass tables in the batch's table block.
+struct BatchLayout {
+  size_t x, b, r, p, ap, rz, phase, it, tol, bytes;
+};
+BatchLayout batch_layout(size_t off, int64_t k) {
+  BatchLayout B;
+  size_t o = off;
+  auto take = [&](size_t n) {
+    o = (o + 15) & ~size_t(15);
+    size_t r = o;
+    o += n;
+    return r;
+  };
+  B.x = take(8 * k);
+  B.b = take(8 * k);
+  B.r = take(8 * k);
+  B.p = take(8 * k);
+  B.ap = take(8 * k);
+  B.rz = take(8 * k);
+  B.phase = take(4 * k);
+  B.it = take(4 * k);
+  B.tol = take(8 * k);
+  B.bytes = (o + 255) & ~size_t(255);
+  return B;
+}
+
+struct BatchCarve {
+  float2* spill;
+  char* tables;
+  TableLayout L;   // pass tables for the full capacity (a smaller member set uses a prefix layout)
+  BatchLayout B;   // member arrays, after the pass tables
+  float2 *r, *p, *ap;
+  double *rz, *pap, *rr;
+  int* status;
+};
+BatchCarve carve_batch(Arena& ar, const hb_plan* p, int64_t K, int64_t S) {
+  BatchCarve c{};
+  const size_t nv = (size_t)image_elems(p);
+  c.spill = ar.take<float2>((size_t)S * spill_elems_per_slot(p));
+  c.L = table_layout(K, S);
+  c.B = batch_layout(c.L.bytes, K);
+  c.tables = ar.take<char>(c.B.bytes);
+  c.r = ar.take<float2>(K * nv);
+  c.p = ar.take<float2>(K * nv);
+  c.ap = ar.take<float2>(K * nv);
+  c.rz = ar.take<double>(2 * K);
+  c.pap = ar.take<double>(K * (size_t)npap_blocks(p));
+  c.rr = ar.take<double>(K * (size_t)nrr_blocks(p));
+  c.status = ar.take<int>(K);
+  return c;
+}
+
+}  // namespace
+
+struct hb_cg_batch {
+  struct Member {
+    bool used = false;
+    int64_t handle = -1;
+    hb_system sys{};
+    std::vector<int64_t> coils;
+    int iters = 0;      // iteration budget
+    double tol = 0.0;
+    int phase = 0;      // 1: initialise at the next step, 2: iterating
+    int it = 0;         // iterations completed
+  };
+  const hb_plan* plan = nullptr;
+  int64_t max_sys = 0, max_slots = 0;
+  BatchCarve c{};
+  std::vector<Member> m;
+  int64_t next_handle = 0;
+  int64_t coils_in_use = 0;
+  std::vector<int64_t> fin_handle;
+  std::vector<int32_t> fin_status, fin_iters;
+};
+
+namespace {
+
 int normal_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, void* ws, size_t ws_bytes,
                         cudaStream_t st) {
   if (int r = validate_systems(p, nsys, sys, false)) return r;
@@ -701,6 +790,7 @@ int normal_systems_impl(const hb_plan* p, int64_t nsys, const hb_system* sys, vo
     const int64_t g = next_group(p, sys, s0, nsys, 0, false, ws_bytes, &slots);
     if (!ws || group_bytes(p, g, slots, 0, false) > ws_bytes)
       return fail(HB_ERR_WORKSPACE, "hb_sense_normal_apply: workspace too small for one system");
+    if (!ws_aligned(ws)) return fail(HB_ERR_INVALID, "hb_sense_normal_apply: workspace not 16-byte aligned");
     Arena ar(ws);
     GroupWs w = carve_group(ar, p, g, slots, 0, false);
     if (int r = upload_tables(p, w, sys, s0, g, false, st)) return r;
@@ -835,6 +925,8 @@ int hb_plan_create(hb_plan** out, int64_t nz, int64_t ny, int64_t nx, int device
   h.insert(h.end(), himg.begin(), himg.end());
   cudaError_t e = cudaMalloc(&p->tables, h.size() * sizeof(float2));
   if (e == cudaSuccess) e = cudaMemcpy(p->tables, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice);
+  // the device's flag for a pass that gave up waiting (bulk copies, tensor-core operands)
+  if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p->tc_wait_error, g_tc_wait_error);
   if (e != cudaSuccess) {
     if (p->tables) cudaFree(p->tables);
     delete p;
@@ -868,7 +960,6 @@ int hb_plan_set_precision(hb_plan* p, int precision) {
     const std::vector<uint16_t> t = tc_dft_table(p->N2);
     cudaError_t e = cudaMalloc(&p->tc_ftab, t.size() * sizeof(uint16_t));
     if (e == cudaSuccess) e = cudaMemcpy(p->tc_ftab, t.data(), t.size() * sizeof(uint16_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p->tc_wait_error, g_tc_wait_error);
     if (e != cudaSuccess) {
       if (p->tc_ftab) cudaFree(p->tc_ftab);
       p->tc_ftab = nullptr;
@@ -995,8 +1086,10 @@ int hb_toeplitz_apply(const hb_plan* p, const void* in, void* out, int64_t out_l
                       int accumulate, const float* packed_diag, void* ws, size_t ws_bytes, void* stream) {
   if (int r = check_plan(p)) return r;
   if (!in || !out || !packed_diag) return fail(HB_ERR_INVALID, "hb_toeplitz_apply: NULL pointer");
+  if (!diag_aligned(packed_diag)) return fail(HB_ERR_INVALID, "hb_toeplitz_apply: packed diagonal not 16-byte aligned");
   if (!ws || ws_bytes < hb_normal_workspace_bytes(p, 1, 1))
     return fail(HB_ERR_WORKSPACE, "hb_toeplitz_apply: workspace too small");
+  if (!ws_aligned(ws)) return fail(HB_ERR_INVALID, "hb_toeplitz_apply: workspace not 16-byte aligned");
   DeviceGuard dg(p->device);
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t coil0 = 0;
@@ -1064,12 +1157,208 @@ int hb_cg_run_systems(const hb_plan* p, int64_t nsys, const hb_system* systems, 
                          (cudaStream_t)stream);
 }
 
+size_t hb_cg_batch_workspace_bytes(const hb_plan* p, int64_t max_systems, int64_t max_coil_slots) {
+  if (!p || max_systems < 1 || max_coil_slots < 1) return 0;
+  Arena ar(nullptr);
+  carve_batch(ar, p, max_systems, max_coil_slots);
+  return ar.off + 256;
+}
+
+int hb_cg_batch_create(hb_cg_batch** out, const hb_plan* p, int64_t max_systems, int64_t max_coil_slots, void* ws,
+                       size_t ws_bytes) {
+  if (!out) return fail(HB_ERR_INVALID, "hb_cg_batch_create: output pointer is NULL");
+  *out = nullptr;
+  if (int r = check_plan(p)) return r;
+  if (max_systems < 1 || max_coil_slots < 1 || max_systems > 65535 || max_coil_slots > 65535)
+    return fail(HB_ERR_INVALID, "hb_cg_batch_create: capacity out of range");
+  if (!ws || ws_bytes < hb_cg_batch_workspace_bytes(p, max_systems, max_coil_slots))
+    return fail(HB_ERR_WORKSPACE, "hb_cg_batch_create: workspace too small");
+  if (!ws_aligned(ws)) return fail(HB_ERR_INVALID, "hb_cg_batch_create: workspace not 16-byte aligned");
+  hb_cg_batch* e = new hb_cg_batch();
+  e->plan = p;
+  e->max_sys = max_systems;
+  e->max_slots = max_coil_slots;
+  Arena ar(ws);
+  e->c = carve_batch(ar, p, max_systems, max_coil_slots);
+  e->m.resize((size_t)max_systems);
+  *out = e;
+  return HB_OK;
+}
+
+int hb_cg_batch_destroy(hb_cg_batch* e) {
+  delete e;
+  return HB_OK;
+}
+
+int hb_cg_batch_add(hb_cg_batch* e, const hb_system* sys, int iters, double tol, int64_t* handle) {
+  if (!e || !sys || !handle) return fail(HB_ERR_INVALID, "hb_cg_batch_add: NULL pointer");
+  if (int r = validate_systems(e->plan, 1, sys, true)) return r;
+  if (sys->precond) return fail(HB_ERR_UNSUPPORTED, "hb_cg_batch_add: preconditioned systems run in hb_cg_run_systems");
+  if (iters < 1) return fail(HB_ERR_INVALID, "hb_cg_batch_add: iters must be >= 1");
+  int64_t k = -1;
+  for (int64_t i = 0; i < e->max_sys && k < 0; ++i)
+    if (!e->m[i].used) k = i;
+  if (k < 0 || e->coils_in_use + sys->ncoil > e->max_slots)
+    return fail(HB_ERR_WORKSPACE, "hb_cg_batch_add: the batch is full (retire finished systems first)");
+  hb_cg_batch::Member& q = e->m[k];
+  q = hb_cg_batch::Member();
+  q.used = true;
+  q.handle = e->next_handle++;
+  q.sys = *sys;
+  q.coils.assign(sys->coils, sys->coils + sys->ncoil);
+  q.sys.coils = q.coils.data();
+  q.iters = iters;
+  q.tol = tol;
+  q.phase = 1;
+  e->coils_in_use += sys->ncoil;
+  *handle = q.handle;
+  return HB_OK;
+}
+
+int hb_cg_batch_step(hb_cg_batch* e, void* stream, int64_t* in_batch) {
+  if (!e) return fail(HB_ERR_INVALID, "hb_cg_batch_step: NULL batch");
+  const hb_plan* p = e->plan;
+  DeviceGuard dg(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<int64_t> mem;  // capacity slots of the members, in slot order
+  int64_t slots = 0;
+  for (int64_t k = 0; k < e->max_sys; ++k)
+    if (e->m[k].used) {
+      mem.push_back(k);
+      slots += e->m[k].sys.ncoil;
+    }
+  const int64_t g = (int64_t)mem.size();
+  if (in_batch) *in_batch = g;
+  if (g == 0) return HB_OK;
+  const size_t nv = (size_t)image_elems(p);
+  // pass tables of the member set (normal-op input: x when initialising, p otherwise;
+  // output: Ap), then the member arrays
+  GroupWs w{};
+  w.spill = e->c.spill;
+  w.tables = e->c.tables;
+  w.L = table_layout(g, slots);
+  std::vector<hb_system> q(g);
+  for (int64_t i = 0; i < g; ++i) {
+    const hb_cg_batch::Member& mm = e->m[mem[i]];
+    q[i] = mm.sys;
+    q[i].x = mm.phase == 1 ? mm.sys.x : (void*)(e->c.p + mem[i] * nv);
+    q[i].out = e->c.ap + mem[i] * nv;
+  }
+  std::vector<char> h(e->c.B.bytes);
+  fill_group_tables(h.data(), p, w, q.data(), 0, g, false);
+  const BatchLayout& B = e->c.B;
+  for (int64_t i = 0; i < g; ++i) {
+    const int64_t k = mem[i];
+    const hb_cg_batch::Member& mm = e->m[k];
+    auto put = [&](size_t off, size_t sz, const void* v) { std::memcpy(h.data() + off + sz * i, v, sz); };
+    void* xp = mm.sys.x;
+    const void* bp = mm.sys.b;
+    void* rp = e->c.r + k * nv;
+    void* pp = e->c.p + k * nv;
+    void* app = e->c.ap + k * nv;
+    void* rzp = e->c.rz + 2 * k;
+    const int ph = mm.phase, it = mm.it;
+    const double tl = mm.tol;
+    put(B.x, 8, &xp);
+    put(B.b, 8, &bp);
+    put(B.r, 8, &rp);
+    put(B.p, 8, &pp);
+    put(B.ap, 8, &app);
+    put(B.rz, 8, &rzp);
+    put(B.phase, 4, &ph);
+    put(B.it, 4, &it);
+    put(B.tol, 8, &tl);
+  }
+  HB_CUDA(cudaMemcpyAsync(e->c.tables, h.data(), B.bytes, cudaMemcpyHostToDevice, st));
+  PassArgs a = group_pass_args(p, w, g, slots, false);
+  a.dot_partials = e->c.pap;  // Re<p, Ap> partials, per member
+  if (int r = run_normal(p, a, st)) return r;
+  CgBatchState s{};
+  s.nmem = (int)g;
+  s.nv = (long long)nv;
+  const char* t = e->c.tables;
+  s.x = (float2* const*)(t + B.x);
+  s.b = (const float2* const*)(t + B.b);
+  s.r = (float2* const*)(t + B.r);
+  s.p = (float2* const*)(t + B.p);
+  s.ap = (const float2* const*)(t + B.ap);
+  s.rz = (double* const*)(t + B.rz);
+  s.phase = (const int*)(t + B.phase);
+  s.it = (const int*)(t + B.it);
+  s.tol = (const double*)(t + B.tol);
+  s.status = e->c.status;
+  s.pap_part = e->c.pap;
+  s.npap = npap_blocks(p);
+  s.rr_part = e->c.rr;
+  const dim3 ugrid(nrr_blocks(p), (unsigned)g);
+  {
+    LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
+    cg_batch_xr_kernel<<<ugrid, 256, 0, st>>>(s);
+  }
+  HB_CHECK_LAUNCH();
+  {
+    LaunchScope ls(HB_KERNEL_CG_UPDATE, st);
+    cg_batch_p_kernel<<<ugrid, 256, 0, st>>>(s);
+  }
+  HB_CHECK_LAUNCH();
+  std::vector<int> stat(g);
+  HB_CUDA(cudaMemcpyAsync(stat.data(), e->c.status, g * sizeof(int), cudaMemcpyDeviceToHost, st));
+  HB_CUDA(cudaStreamSynchronize(st));  // the host image of the tables is reused next step
+  if (int r = tc_wait_check()) return r;
+  // advance every member; finished ones leave the batch
+  int64_t left = 0;
+  for (int64_t i = 0; i < g; ++i) {
+    hb_cg_batch::Member& mm = e->m[mem[i]];
+    int done_status = -1;
+    if (mm.phase == 1) {
+      if (stat[i] == kCgConverged) done_status = HB_CG_CONVERGED;
+      mm.phase = 2;
+      mm.it = 0;
+    } else if (stat[i] == kCgNotPD) {
+      done_status = HB_CG_NOT_PD;
+    } else {
+      mm.it += 1;
+      if (stat[i] == kCgConverged) done_status = HB_CG_CONVERGED;
+      else if (mm.it >= mm.iters) done_status = HB_CG_RUNNING;
+    }
+    if (done_status >= 0) {
+      e->fin_handle.push_back(mm.handle);
+      e->fin_status.push_back(done_status);
+      e->fin_iters.push_back(mm.it);
+      e->coils_in_use -= mm.sys.ncoil;
+      mm = hb_cg_batch::Member();
+    } else {
+      ++left;
+    }
+  }
+  if (in_batch) *in_batch = left;
+  return HB_OK;
+}
+
+int hb_cg_batch_retire(hb_cg_batch* e, int64_t* handles, int32_t* status, int32_t* iters, int64_t cap,
+                       int64_t* n_out) {
+  if (!e || !n_out) return fail(HB_ERR_INVALID, "hb_cg_batch_retire: NULL pointer");
+  const int64_t n = std::min<int64_t>(cap, (int64_t)e->fin_handle.size());
+  for (int64_t i = 0; i < n; ++i) {
+    if (handles) handles[i] = e->fin_handle[i];
+    if (status) status[i] = e->fin_status[i];
+    if (iters) iters[i] = e->fin_iters[i];
+  }
+  e->fin_handle.erase(e->fin_handle.begin(), e->fin_handle.begin() + n);
+  e->fin_status.erase(e->fin_status.begin(), e->fin_status.begin() + n);
+  e->fin_iters.erase(e->fin_iters.begin(), e->fin_iters.begin() + n);
+  *n_out = n;
+  return HB_OK;
+}
+
 int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in, void* out, int64_t out_ldz,
                               int64_t out_ldy, const void* mul, int accumulate, const float* packed_diag,
                               void* stream) {
   if (!hb_size_supported(nz, ny, nx))
     return fail(HB_ERR_UNSUPPORTED, "hb_toeplitz_apply_noalloc: image size not supported");
   if (!in || !out || !packed_diag) return fail(HB_ERR_INVALID, "hb_toeplitz_apply_noalloc: NULL pointer");
+  if (!diag_aligned(packed_diag))
+    return fail(HB_ERR_INVALID, "hb_toeplitz_apply_noalloc: packed diagonal not 16-byte aligned");
   const unsigned long long need = 16ull * (unsigned long long)(nz * ny * nx);
   if (need > HB_NOALLOC_SCRATCH_BYTES)
     return fail(HB_ERR_WORKSPACE, "hb_toeplitz_apply_noalloc: " + std::to_string(nz) + "x" + std::to_string(ny) + "x" +
@@ -1160,6 +1449,7 @@ int hb_plan_autotune(hb_plan* p, int64_t nslots, void* ws, size_t ws_bytes, void
   if (nslots < 1 || nslots > 65535) return fail(HB_ERR_INVALID, "hb_plan_autotune: nslots");
   if (!ws || ws_bytes < hb_autotune_workspace_bytes(p, nslots))
     return fail(HB_ERR_WORKSPACE, "hb_plan_autotune: workspace too small");
+  if (!ws_aligned(ws)) return fail(HB_ERR_INVALID, "hb_plan_autotune: workspace not 16-byte aligned");
   DeviceGuard dg(p->device);
   cudaStream_t st = (cudaStream_t)stream;
   int nvar = 0;

@@ -196,4 +196,110 @@ __global__ void __launch_bounds__(256) cg_precond_scale_kernel(CgState s) {
 // Ends an iteration: every kernel of the next one reads the advanced counter.
 __global__ void cg_advance_kernel(int* iter) { *iter += 1; }
 
+// ------------------------------------------------------------ running batch (engine) ----
+// A running batch holds systems at different points of their solves: a member that joined
+// at this iteration boundary initialises (phase 1: r = b - A x, p = r, rz = Re<r, r>) while
+// the others take one iteration (phase 2), in the same launches.  The host owns each
+// member's phase and iteration number and uploads them with the member tables before the
+// step; rz of capacity slot k lives in rz[k][0..1], iteration i reading rz[k][i & 1] and
+// writing rz[k][(i + 1) & 1], so no kernel reads what another CTA of it writes.  The
+// arithmetic of an iteration is that of cg_step_xr_kernel / cg_step_p_kernel (same
+// operands, same order), so a member's iterates are bitwise those of hb_cg_run_systems.
+struct CgBatchState {
+  int nmem;
+  long long nv;
+  float2* const* x;        // [nmem] solution (caller buffer)
+  const float2* const* b;  // [nmem] right-hand side (caller buffer)
+  float2* const* r;        // [nmem] capacity-slot vectors
+  float2* const* p;
+  const float2* const* ap;
+  double* const* rz;       // [nmem] -> rz pair of the member's capacity slot
+  const int* phase;        // [nmem] 1 = initialise, 2 = iterate
+  const int* it;           // [nmem] iteration index (phase 2)
+  const double* tol;       // [nmem]
+  int* status;             // [nmem] out: kCgRunning / kCgConverged / kCgNotPD
+  const double* pap_part;  // [nmem][npap] partials of Re<p, Ap> (pass C)
+  int npap;
+  double* rr_part;         // [nmem][gridDim.x]
+};
+
+// phase 1: r = b - Ap, p = r;  phase 2: the x/r update of cg_step_xr_kernel.  Partials of
+// Re<r, r> either way.
+__global__ void __launch_bounds__(256) cg_batch_xr_kernel(CgBatchState s) {
+  __shared__ double red[32];
+  const int m = blockIdx.y;
+  float2* r = s.r[m];
+  float2* p = s.p[m];
+  const float2* ap = s.ap[m];
+  double acc = 0.0;
+  if (s.phase[m] == 1) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.status[m] = kCgRunning;
+    const float2* b = s.b[m];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv;
+         i += (long long)gridDim.x * blockDim.x) {
+      const float2 v = csub(b[i], ap[i]);
+      r[i] = v;
+      p[i] = v;
+      acc += (double)v.x * v.x + (double)v.y * v.y;
+    }
+  } else {
+    const double pap = block_sum_fixed(s.pap_part + (long long)m * s.npap, s.npap, red);
+    if (!(pap > 0.0)) {  // also catches NaN
+      if (blockIdx.x == 0 && threadIdx.x == 0) s.status[m] = kCgNotPD;
+      return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.status[m] = kCgRunning;
+    const double alpha = s.rz[m][s.it[m] & 1] / pap;
+    const float af = (float)alpha;
+    float2* xv = s.x[m];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv;
+         i += (long long)gridDim.x * blockDim.x) {
+      const float2 pv = p[i];
+      const float2 apv = ap[i];
+      float2 xx = xv[i];
+      float2 rr = r[i];
+      xx.x = fmaf(af, pv.x, xx.x);
+      xx.y = fmaf(af, pv.y, xx.y);
+      rr.x = fmaf(-af, apv.x, rr.x);
+      rr.y = fmaf(-af, apv.y, rr.y);
+      xv[i] = xx;
+      r[i] = rr;
+      acc += (double)rr.x * rr.x + (double)rr.y * rr.y;
+    }
+  }
+  block_write_partial(acc, s.rr_part + (long long)m * gridDim.x + blockIdx.x, red);
+}
+
+// phase 1: rz[0] = Re<r, r>, converged if below tol;  phase 2: the p update of
+// cg_step_p_kernel, rz of the next iteration, converged if below tol.
+__global__ void __launch_bounds__(256) cg_batch_p_kernel(CgBatchState s) {
+  __shared__ double red[32];
+  const int m = blockIdx.y;
+  if (s.status[m] == kCgNotPD) return;  // written by cg_batch_xr_kernel, complete
+  const double rznew = block_sum_fixed(s.rr_part + (long long)m * gridDim.x, gridDim.x, red);
+  if (s.phase[m] == 1) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      s.rz[m][0] = rznew;
+      if (sqrt(rznew) < s.tol[m]) s.status[m] = kCgConverged;
+    }
+    return;
+  }
+  const int it = s.it[m];
+  const double rzold = s.rz[m][it & 1];
+  const float beta = (float)(rznew / rzold);
+  float2* p = s.p[m];
+  const float2* r = s.r[m];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.nv; i += (long long)gridDim.x * blockDim.x) {
+    const float2 rv = r[i];
+    float2 pv = p[i];
+    pv.x = fmaf(beta, pv.x, rv.x);
+    pv.y = fmaf(beta, pv.y, rv.y);
+    p[i] = pv;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s.rz[m][(it + 1) & 1] = rznew;
+    if (sqrt(rznew) < s.tol[m]) s.status[m] = kCgConverged;
+  }
+}
+
 }  // namespace hb

@@ -12,6 +12,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "fft.cuh"
 
 namespace hb {
 
@@ -129,9 +130,12 @@ __global__ void diag_to_complex_kernel(const double2* __restrict__ acc, long lon
   T[i] = make_float2((float)(acc[i].x * scale), (float)(acc[i].y * scale));
 }
 
-// Pack Re(T) into the layout pass B reads: packed[kx][h][ky'][kz] (ky = 2*ky' + h),
-// scaled by `scale` (the inverse-FFT factor 1/prod(M), plus any psf scaling).
-// Source is either a float2 reference-layout T or a double2 accumulator.
+// Pack Re(T) into the layout pass B reads: packed[kx][h][ky'][p] (ky = 2*ky' + h), one
+// M0-long column per (kx, ky) in the order the z transform's lanes consume it: position
+// p = t*E + r holds kz = dout_index<M0>(t, r) (lane t's E values are contiguous, so a lane
+// fetches them with 16-byte loads).  Scaled by `scale` (the inverse-FFT factor 1/prod(M),
+// plus any psf scaling).  Source is either a float2 reference-layout T or a double2
+// accumulator.
 template <typename Src>
 __global__ void diag_pack_kernel(const Src* __restrict__ T, int M0, int M1, int M2, double scale,
                                  float* __restrict__ packed) {
@@ -139,7 +143,7 @@ __global__ void diag_pack_kernel(const Src* __restrict__ T, int M0, int M1, int 
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   // i enumerates the packed layout
-  const int kz = (int)(i % M0);
+  const int kz = column_kz(M0, (int)(i % M0));
   long long r = i / M0;
   const int N1 = M1 / 2;
   const int kyh = (int)(r % N1);

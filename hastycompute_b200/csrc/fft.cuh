@@ -399,6 +399,33 @@ __device__ __forceinline__ void team_fft_dout_to_din_r(float2* v, int t, float2*
   (void)HALF_OUT;
 }
 
+// Team shape (E, S) of a line of length L at run time (the TeamCfg table).
+__host__ __device__ inline void team_shape(int L, int* E, int* S) {
+  switch (L) {
+    case 8: *E = 4; *S = 2; return;
+    case 16: *E = 4; *S = 4; return;
+    case 32: *E = 8; *S = 4; return;
+    case 64: *E = 8; *S = 8; return;
+    case 128: *E = 16; *S = 8; return;
+    case 256: *E = 16; *S = 16; return;
+    case 96: *E = 24; *S = 4; return;
+    case 160: *E = 40; *S = 4; return;
+    case 192: *E = 24; *S = 8; return;
+    case 320: *E = 40; *S = 8; return;
+    case 512: *E = 32; *S = 16; return;
+    default: *E = L; *S = 1; return;
+  }
+}
+
+// The frequency a z-column position p = t*E + r holds in the packed diagonal: the output
+// index dout_index<L>(t, r) = (t + S*(r/S)) + E*(r%S) of lane t, register r.
+__host__ __device__ inline int column_kz(int L, int p) {
+  int E, S;
+  team_shape(L, &E, &S);
+  const int t = p / E, r = p % E;
+  return (t + S * (r / S)) + E * (r % S);
+}
+
 // Index helpers for the two layouts.
 template <int L>
 HB_DEV int din_index(int t, int e) { return t + TeamCfg<L>::S * e; }

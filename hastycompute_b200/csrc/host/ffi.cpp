@@ -108,6 +108,27 @@ class BatchedSenseNormalToeplitz : public torch::CustomClassHolder {
     return std::vector<int64_t>(solver.iterations().begin(), solver.iterations().end());
   }
 
+  // Preconditioned CG: as cg, with P = CirculantPreconditionerOp::Create(precond, centered,
+  // nullopt, false) (batch_sense.ixx:388-390 builds it that way); precond is the diagonal
+  // of CirculantPreconditionerOp::build_diagonal (centred) or, with centered = false, in FFT
+  // order.  A real diagonal runs the device PCG.
+  std::vector<int64_t> pcg(at::Tensor x, const at::Tensor& b, int64_t iters, double tol, double lambda,
+                           const std::optional<std::vector<int64_t>>& coils, const at::Tensor& precond,
+                           bool centered) {
+    std::vector<int64_t> cl;
+    if (coils.has_value()) {
+      cl = *coils;
+    } else {
+      for (int64_t c = 0; c < _op->smaps().size(0); ++c) cl.push_back(c);
+    }
+    auto A = std::make_shared<op::SenseNormalToeplitzOp>(_op, cl, lambda);
+    std::shared_ptr<op::Operator> P = mri::CirculantPreconditionerOp::Create(precond, centered, std::nullopt, false);
+    op::Vector xv(x);
+    op::ConjugateGradient solver(A, std::make_shared<op::Vector>(b), P);
+    solver.run(xv, (int)iters, tol);
+    return std::vector<int64_t>(solver.iterations().begin(), solver.iterations().end());
+  }
+
  private:
   std::vector<std::vector<int64_t>> all_coils(const at::Tensor& in) const {
     const auto& d = _op->plan()->image_dims();
@@ -154,7 +175,13 @@ TORCH_LIBRARY(HastyToeplitz, m) {
       .def("apply", &hasty::ffi::BatchedSenseNormalToeplitz::apply)
       .def("apply_regularized", &hasty::ffi::BatchedSenseNormalToeplitz::apply_regularized)
       .def("set_precision", &hasty::ffi::BatchedSenseNormalToeplitz::set_precision)
-      .def("cg", &hasty::ffi::BatchedSenseNormalToeplitz::cg);
+      .def("cg", &hasty::ffi::BatchedSenseNormalToeplitz::cg)
+      .def("pcg", &hasty::ffi::BatchedSenseNormalToeplitz::pcg);
+
+  m.def("circulant_precond_diagonal",
+        [](const at::Tensor& smaps, const at::Tensor& coord, double lambda) {
+          return hasty::mri::CirculantPreconditionerOp::build_diagonal(smaps, coord, std::nullopt, lambda);
+        });
 
   m.def("batched_sense_toeplitz_diagonals", &hasty::ffi::batched_sense_toeplitz_diagonals);
 }

@@ -12,6 +12,7 @@
 //   hasty::op::Vector / Operator              lib/op/vec.ixx:39-119, lib/op/op.ixx:30-109
 //   hasty::op::ConjugateGradient              lib/op/opalgs.ixx:36-47, opalgs.cpp:50-96
 //   hasty::op::BatchedConjugateGradient       lib/op/opalgs.ixx:84-136
+//   hasty::mri::CirculantPreconditionerOp     lib/mri/precond.ixx:13-37, precond.cpp:17-117
 #pragma once
 
 #include <ATen/ATen.h>
@@ -208,10 +209,58 @@ class SenseNormalToeplitzOp : public Operator {
   double _lambda;
 };
 
+}  // namespace op
+
+namespace mri {
+
+// Drop-in for hasty::mri::CirculantPreconditionerOp (precond.ixx:13-37, precond.cpp:17-63):
+//   P x = ifft(D * fft(x))                       (centered = false)
+//   P x = ifftc(D * fftc(x))                     (centered = true)
+//   adjointify: fft(conj(D) * ifft(x)), resp. fftc(conj(D) * ifftc(x)).
+// norm may be absent, "backward", "ortho" or "forward" (the pair's scaling is 1/N for all
+// three).  When D is real and the image size is one the kernels support, the operator is
+// also held as the real float32 diagonal in FFT order that the device PCG reads (for even
+// sizes ifftc(D * fftc(x)) = ifft(ifftshift(D) * fft(x)), and for real D the adjointified
+// form is the same operator with D index-reversed), and apply() runs hb_precond_apply.
+// Otherwise apply() runs the reference's ATen calls.
+class CirculantPreconditionerOp : public op::Operator {
+ public:
+  static std::unique_ptr<CirculantPreconditionerOp> Create(at::Tensor diag, bool centered,
+                                                           const std::optional<std::string>& norm, bool adjointify);
+  // precond.cpp:65-117 (ported from sigpy there): 1 / (d + lambda), d the Fourier-domain
+  // diagonal of sum_c S_c^H (A^H A)_toep S_c for the trajectory coord [3, K] float32,
+  // built on the device by hb_precond_build (tol 1e-6); returned in the centred layout,
+  // float32 [nz, ny, nx], the form the reference's loaders pass to Create(diag, true, ...)
+  // (batch_sense.ixx:388-390).  Sample weights are not supported (std::runtime_error).
+  static at::Tensor build_diagonal(at::Tensor smaps, at::Tensor coord,
+                                   const std::optional<at::Tensor>& weights = std::nullopt,
+                                   const std::optional<double>& lambda = 0.0);
+  op::Vector apply(const op::Vector& in) const override;
+  // Real float32 [nz, ny, nx] diagonal in FFT order for the device PCG; undefined tensor
+  // when the operator has no such form.
+  const at::Tensor& fft_order_diagonal() const { return _fftdiag; }
+
+ protected:
+  CirculantPreconditionerOp(at::Tensor diag, bool centered, const std::optional<std::string>& norm, bool adjointify);
+
+ private:
+  at::Tensor _diag;
+  bool _centered;
+  std::optional<std::string> _norm;
+  bool _adjointify;
+  at::Tensor _fftdiag;
+  std::shared_ptr<detail::Plan> _plan;
+};
+
+}  // namespace mri
+
+namespace op {
+
 // ConjugateGradient(A, b, P).run(x, iter, tol)  (opalgs.cpp:50-96).
-// With A a SenseNormalToeplitzOp and no preconditioner the whole solve (all systems of
-// x) runs on the device (fused updates, FP64 reductions, no per-iteration host sync).
-// Any other operator runs the reference recurrences on ATen tensors.
+// With A a SenseNormalToeplitzOp and P absent or a CirculantPreconditionerOp with a real
+// diagonal, the whole solve (all systems of x) runs on the device (fused updates, FP64
+// reductions, no per-iteration host sync; preconditioned CG when P is given).  Any other
+// operator runs the reference recurrences on ATen tensors.
 class ConjugateGradient {
  public:
   ConjugateGradient(sptr<Operator> A, sptr<Vector> b, sptr<Operator> P);

@@ -432,34 +432,69 @@ Vector SenseNormalToeplitzOp::apply(const Vector& in) const {
 ConjugateGradient::ConjugateGradient(sptr<Operator> A, sptr<Vector> b, sptr<Operator> P)
     : _A(std::move(A)), _b(std::move(b)), _P(std::move(P)) {}
 
+namespace {
+// Device form (real float32, FFT order, on the plan's device) of a preconditioner for the
+// fused PCG, or an undefined tensor when P has none (or is absent).
+at::Tensor device_precond(const sptr<Operator>& P, const detail::Plan& plan) {
+  auto circ = std::dynamic_pointer_cast<mri::CirculantPreconditionerOp>(P);
+  if (!circ || !circ->fft_order_diagonal().defined()) return at::Tensor();
+  const auto& d = plan.image_dims();
+  const at::Tensor& f = circ->fft_order_diagonal();
+  if (f.numel() != d[0] * d[1] * d[2]) return at::Tensor();
+  return f.to(plan.device(), at::kFloat).contiguous();
+}
+
+// The whole (P)CG of every system of x on the device: hb_cg_run_systems with system i's
+// diagonal and precond[i] (undefined = plain CG for that system, or one entry for all).
+void device_cg(const SenseNormalToeplitzOp& top, Vector& x, const Vector& b, const std::vector<at::Tensor>& precond,
+               int iter, double tol, std::vector<int32_t>& status, std::vector<int32_t>& iters) {
+  const auto& bat = *top.batched();
+  const auto& plan = *bat.plan();
+  at::Tensor xs = gather_systems(x, plan);
+  at::Tensor bs = gather_systems(b, plan);
+  const int64_t nsys = xs.size(0);
+  if (bs.size(0) != nsys) throw std::runtime_error("x and b hold different numbers of systems");
+  if (precond.size() != 1 && (int64_t)precond.size() != nsys)
+    throw std::runtime_error("one preconditioner per system (or one for all) is required");
+  const int64_t nv = xs.numel() / std::max<int64_t>(nsys, 1);
+  const int64_t pn = plan.packed_numel();
+  std::vector<hb_system> sys(nsys);
+  for (int64_t i = 0; i < nsys; ++i) {
+    const int64_t di = bat.diag_index().empty() ? (nsys == 1 ? 0 : i) : bat.diag_index()[i];
+    const at::Tensor& pc = precond.size() == 1 ? precond[0] : precond[i];
+    hb_system q{};
+    q.x = (char*)xs.data_ptr() + i * nv * 8;
+    q.b = (const char*)bs.data_ptr() + i * nv * 8;
+    q.smaps = bat.smaps().data_ptr();
+    q.coils = top.coils().data();
+    q.ncoil = (int64_t)top.coils().size();
+    q.packed_diag = bat.packed().data_ptr<float>() + di * pn;
+    q.lambda = (float)top.lambda();
+    q.precond = pc.defined() ? pc.data_ptr<float>() : nullptr;
+    sys[i] = q;
+  }
+  status.assign(nsys, 0);
+  iters.assign(nsys, 0);
+  size_t nb = hb_systems_workspace_bytes(plan.get(), nsys, nsys * (int64_t)top.coils().size(), iter);
+  at::Tensor ws = plan.workspace(nb);
+  int rc = hb_cg_run_systems(plan.get(), nsys, sys.data(), iter, tol, 0, status.data(), iters.data(), ws.data_ptr(),
+                             nb, detail::current_stream(plan.device()));
+  int64_t off = 0;
+  scatter_systems(x, xs, off);
+  detail::check(rc);
+}
+}  // namespace
+
 void ConjugateGradient::run(Vector& x, int iter, double tol) {
   c10::InferenceMode guard;
   if (iter < 1) return;
   auto top = std::dynamic_pointer_cast<SenseNormalToeplitzOp>(_A);
-  if (top && !_P) {
-    const auto& bat = *top->batched();
-    const auto& plan = *bat.plan();
-    const auto& d = plan.image_dims();
-    at::Tensor xs = gather_systems(x, plan);
-    at::Tensor bs = gather_systems(*_b, plan);
-    const int64_t nsys = xs.size(0);
-    if (bs.size(0) != nsys) throw std::runtime_error("x and b hold different numbers of systems");
-    std::vector<int64_t> didx(nsys);
-    for (int64_t i = 0; i < nsys; ++i)
-      didx[i] = bat.diag_index().empty() ? (nsys == 1 ? 0 : i) : bat.diag_index()[i];
-    _status.assign(nsys, 0);
-    _iters.assign(nsys, 0);
-    size_t nb = hb_cg_workspace_bytes(plan.get(), nsys, (int64_t)top->coils().size(), iter);
-    at::Tensor ws = plan.workspace(nb);
-    int rc = hb_cg_run(plan.get(), nsys, xs.data_ptr(), bs.data_ptr(), bat.smaps().data_ptr(), top->coils().data(),
-                       (int64_t)top->coils().size(), bat.packed().data_ptr<float>(), didx.data(),
-                       (float)top->lambda(), iter, tol, _status.data(), _iters.data(), ws.data_ptr(), nb,
-                       detail::current_stream(plan.device()));
-    int64_t off = 0;
-    scatter_systems(x, xs, off);
-    (void)d;
-    detail::check(rc);
-    return;
+  if (top) {
+    at::Tensor pd = device_precond(_P, *top->batched()->plan());
+    if (!_P || pd.defined()) {
+      device_cg(*top, x, *_b, {pd}, iter, tol, _status, _iters);
+      return;
+    }
   }
   // generic operator: the reference recurrences on ATen tensors (opalgs.cpp:50-96)
   Vector r = *_b - _A->apply(x);
@@ -484,6 +519,100 @@ void ConjugateGradient::run(Vector& x, int iter, double tol) {
   }
 }
 
+}  // namespace op
+
+namespace mri {
+
+namespace {
+bool norm_ok(const std::optional<std::string>& n) {
+  return !n.has_value() || *n == "backward" || *n == "ortho" || *n == "forward";
+}
+std::optional<c10::string_view> norm_view(const std::optional<std::string>& n) {
+  return n.has_value() ? std::optional<c10::string_view>(c10::string_view(*n)) : std::nullopt;
+}
+}  // namespace
+
+std::unique_ptr<CirculantPreconditionerOp> CirculantPreconditionerOp::Create(at::Tensor diag, bool centered,
+                                                                             const std::optional<std::string>& norm,
+                                                                             bool adjointify) {
+  return std::unique_ptr<CirculantPreconditionerOp>(
+      new CirculantPreconditionerOp(std::move(diag), centered, norm, adjointify));
+}
+
+CirculantPreconditionerOp::CirculantPreconditionerOp(at::Tensor diag, bool centered,
+                                                     const std::optional<std::string>& norm, bool adjointify)
+    : _diag(std::move(diag)), _centered(centered), _norm(norm), _adjointify(adjointify) {
+  if (!norm_ok(_norm)) throw std::runtime_error("CirculantPreconditionerOp: unknown norm " + *_norm);
+  // the device form: real D over a supported even image size
+  at::Tensor d = _diag;
+  while (d.dim() > 3 && d.size(0) == 1) d = d.squeeze(0);
+  if (d.dim() != 3 || !d.is_cuda()) return;
+  if (d.is_complex()) {
+    if (at::any(at::imag(d) != 0).item<bool>()) return;
+    d = at::real(d);
+  }
+  if (!hb_size_supported(d.size(0), d.size(1), d.size(2))) return;
+  for (int a = 0; a < 3; ++a)
+    if (d.size(a) % 2) return;
+  if (_centered) d = at::fft_ifftshift(d);
+  if (_adjointify) d = at::roll(at::flip(d, {0, 1, 2}), {1, 1, 1}, {0, 1, 2});  // D[-k]
+  _fftdiag = d.to(at::kFloat).contiguous();
+  _plan = std::make_shared<detail::Plan>(std::vector<int64_t>{d.size(0), d.size(1), d.size(2)}, d.device());
+}
+
+op::Vector CirculantPreconditionerOp::apply(const op::Vector& in) const {
+  if (in.has_children()) {
+    std::vector<op::Vector> out;
+    for (const auto& ch : in.children()) out.push_back(apply(ch));
+    return op::Vector(out);
+  }
+  const at::Tensor& x = in.tensor();
+  if (_fftdiag.defined() && x.is_cuda() && x.device() == _fftdiag.device() && x.scalar_type() == at::kComplexFloat &&
+      x.numel() == _fftdiag.numel()) {
+    at::Tensor xc = x.contiguous();
+    at::Tensor y = at::empty_like(xc);
+    detail::check(hb_precond_apply(_plan->get(), _fftdiag.data_ptr<float>(), xc.data_ptr(), y.data_ptr(),
+                                   detail::current_stream(x.device())));
+    return op::Vector(y);
+  }
+  // the reference's own calls (precond.cpp:30-52)
+  auto nv = norm_view(_norm);
+  auto fftc = [&](const at::Tensor& t) { return at::fft_fftshift(at::fft_fftn(at::fft_ifftshift(t), c10::nullopt, c10::nullopt, nv)); };
+  auto ifftc = [&](const at::Tensor& t) { return at::fft_fftshift(at::fft_ifftn(at::fft_ifftshift(t), c10::nullopt, c10::nullopt, nv)); };
+  at::Tensor D = _diag.to(x.device());
+  if (_adjointify) {
+    if (_centered) return op::Vector(fftc(D.conj() * ifftc(x)));
+    return op::Vector(at::fft_fftn(D.conj() * at::fft_ifftn(x, c10::nullopt, c10::nullopt, nv), c10::nullopt,
+                                   c10::nullopt, nv));
+  }
+  if (_centered) return op::Vector(ifftc(D * fftc(x)));
+  return op::Vector(at::fft_ifftn(D * at::fft_fftn(x, c10::nullopt, c10::nullopt, nv), c10::nullopt, c10::nullopt, nv));
+}
+
+at::Tensor CirculantPreconditionerOp::build_diagonal(at::Tensor smaps, at::Tensor coord,
+                                                     const std::optional<at::Tensor>& weights,
+                                                     const std::optional<double>& lambda) {
+  c10::InferenceMode guard;
+  if (weights.has_value()) throw std::runtime_error("CirculantPreconditionerOp::build_diagonal: weights not supported");
+  if (smaps.dim() != 4) throw std::runtime_error("smaps must be [ncoil, nz, ny, nx]");
+  if (coord.dim() != 2 || coord.size(0) != 3) throw std::runtime_error("coord must be [3, nsamples]");
+  const c10::Device dev = smaps.is_cuda() ? smaps.device() : c10::Device(c10::kCUDA, 0);
+  detail::Plan plan({smaps.size(1), smaps.size(2), smaps.size(3)}, dev);
+  at::Tensor sm = smaps.to(dev, at::kComplexFloat).contiguous();
+  at::Tensor c = coord.to(dev, at::kFloat).contiguous();
+  std::vector<int64_t> coils(smaps.size(0));
+  for (int64_t i = 0; i < smaps.size(0); ++i) coils[i] = i;
+  at::Tensor p = at::empty({smaps.size(1), smaps.size(2), smaps.size(3)}, at::TensorOptions().dtype(at::kFloat).device(dev));
+  detail::check(hb_precond_build(plan.get(), c.data_ptr<float>(), c.size(1), 1e-6, sm.data_ptr(), coils.data(),
+                                 (int64_t)coils.size(), (float)lambda.value_or(0.0), p.data_ptr<float>(),
+                                 detail::current_stream(dev)));
+  return at::fft_fftshift(p);
+}
+
+}  // namespace mri
+
+namespace op {
+
 BatchedConjugateGradient::BatchedConjugateGradient(std::vector<ConjugateGradientLoadResult> systems)
     : _systems(std::move(systems)) {}
 
@@ -491,13 +620,23 @@ void BatchedConjugateGradient::run(Vector& x, int iter, double tol) {
   c10::InferenceMode guard;
   auto& children = x.children();
   if (children.size() != _systems.size()) throw std::runtime_error("one load result per child of x is required");
-  // fuse every system whose operator shares the first system's batched Toeplitz op
+  // fuse every system whose operator shares the first system's batched Toeplitz op; each
+  // may carry its own circulant preconditioner (device PCG per system)
   auto first = std::dynamic_pointer_cast<SenseNormalToeplitzOp>(_systems.empty() ? nullptr : _systems[0].A);
   bool fusable = first != nullptr;
+  std::vector<at::Tensor> pre;
   for (const auto& s : _systems) {
     auto t = std::dynamic_pointer_cast<SenseNormalToeplitzOp>(s.A);
-    if (!t || s.P || t->batched() != first->batched() || t->coils() != first->coils() || t->lambda() != first->lambda())
+    if (!t || t->batched() != first->batched() || t->coils() != first->coils() || t->lambda() != first->lambda()) {
       fusable = false;
+      break;
+    }
+    at::Tensor pd = device_precond(s.P, *first->batched()->plan());
+    if (s.P && !pd.defined()) {
+      fusable = false;
+      break;
+    }
+    pre.push_back(pd);
   }
   if (fusable) {
     const auto& bat = *first->batched();
@@ -506,10 +645,15 @@ void BatchedConjugateGradient::run(Vector& x, int iter, double tol) {
     std::vector<Vector> bs;
     for (const auto& s : _systems) bs.push_back(s.b);
     Vector ball(bs);
-    if (count_systems(x, nv) != (int64_t)_systems.size() && bat.diag_index().size() != (size_t)count_systems(x, nv))
-      throw std::runtime_error("each child of x must hold one system");
-    ConjugateGradient cg(first, std::make_shared<Vector>(ball), nullptr);
-    cg.run(x, iter, tol);
+    const int64_t ns = count_systems(x, nv);
+    if (ns != (int64_t)_systems.size()) {
+      if (bat.diag_index().size() != (size_t)ns) throw std::runtime_error("each child of x must hold one system");
+      for (const auto& t : pre)
+        if (t.defined()) throw std::runtime_error("with preconditioners each child of x must hold one system");
+      pre = {at::Tensor()};
+    }
+    std::vector<int32_t> status, iters;
+    device_cg(*first, x, ball, pre, iter, tol, status, iters);
     return;
   }
   for (size_t i = 0; i < _systems.size(); ++i) {

@@ -1,7 +1,8 @@
 // Pass A on the 5th-generation tensor cores (tcgen05): the zero-padded 2nx-point DFT along
 // x as a dense contraction, for nx = ny = 128.
 //
-//   spill[slot][z][kx][y] = sum_{x < nx} F[kx][x] * (S_c * x)[z][y][x],  F[kx][x] = e^{-2 pi i kx x / 2nx}
+//   spill(slot, z, kx, y) = sum_{x < nx} F[kx][x] * (S_c * x)[z][y][x],  F[kx][x] = e^{-2 pi i kx x / 2nx}
+// (stored at spill_index, the tiled layout passes B and C read)
 //
 // One CTA per (slot, z): D^T[y][kx] = A[y][x] . F[kx][x]^T with A = S_c * x (M = 128
 // lines y, N = 256 frequencies kx, K = 128 samples x), so every sample is loaded and split
@@ -51,7 +52,6 @@ constexpr int kThreadsAll = kThreads + 32;  // + warp 8: bulk copies and contrac
 constexpr int kTmemCols = 2 * kCols;       // D_re [0, 256), D_im [256, 512)
 constexpr int kSmemBytes = kStagesA * kStageA + kStagesF * kStageF;  // 160 KB
 static_assert(kFAhead + kStagesA <= kStagesF, "the F slot refilled at chunk kc was freed by chunk kc - kStagesA");
-constexpr long long kWaitCycles = 2000000000LL;  // about one second of SM clocks
 
 // Byte offset of element (row r, k) in a [rows][16] K-major operand array without swizzle:
 // core matrices of 8 rows x 16 bytes; the two 8-element K halves of an 8-row group are
@@ -81,46 +81,9 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
          ((uint64_t)((kSbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Waits for the phase of the given parity to complete; false after kWaitCycles or once
-// another thread of the CTA has raised *abort.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* abort) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity))
-    if (*abort || clock64() - t0 > kWaitCycles) return false;
-  return true;
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
 __device__ __forceinline__ void st_shared_b32(uint32_t addr, uint32_t v) {
   asm volatile("st.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -354,7 +317,8 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 1) expand_fwd_x_tc_kernel(Pas
       // epilogue: warp w reads TMEM lanes [32 (w % 4), +32) = lines y, columns (kx) of half w / 4
       const int q = warp % 4, ch = warp / 4;
       const int y = q * 32 + lane;
-      float2* dst = a.spill + spill_offset(slot, z, 0, N0, N1, M2) + y;
+      constexpr int YT = spill_yt(kRows);
+      float2* dst = a.spill + spill_tile_offset(slot, z, y / YT, N0, N1, M2);  // y's spill tile
 #pragma unroll 1
       for (int cb = 0; cb < kCols / 32; ++cb) {
         const int c0 = ch * (kCols / 2) + cb * 16;
@@ -364,7 +328,7 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 1) expand_fwd_x_tc_kernel(Pas
         tmem_ld_wait();
 #pragma unroll
         for (int j = 0; j < 16; ++j)
-          dst[(long long)(c0 + j) * N1] = make_float2(__uint_as_float(re[j]), __uint_as_float(im[j]));
+          dst[spill_in_tile(c0 + j, y % YT, YT)] = make_float2(__uint_as_float(re[j]), __uint_as_float(im[j]));
       }
     }
   }

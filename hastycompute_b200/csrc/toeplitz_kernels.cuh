@@ -21,14 +21,56 @@
 
 #include <cooperative_groups.h>
 
+#include "bulk.cuh"
 #include "common.cuh"
 #include "fft.cuh"
 
 namespace hb {
 
+// ------------------------------------------------------------------- spill layout ----
+// The spill holds, per (system, coil) slot, the image after the forward x transform:
+// [slot][z][yt][kx][yy'] with yt = y / YT, yy' = (y % YT) ^ (kx % YT), YT = spill_yt(N1).
+// * The (slot, z, yt) tile that passes A and C move is one contiguous M2 x YT block, so it
+//   travels as one bulk copy and lies in shared memory exactly as in global memory.
+// * The XOR puts the YT values of one kx row in an order that depends on kx, so a tile
+//   column (one y, consecutive kx: what one FFT team writes or reads) falls on distinct
+//   shared-memory banks without padding.
+// * Row z of the (slot, kx) plane that pass B transforms is N1 / YT chunks of YT values
+//   (128 bytes for YT = 16), M2 * YT apart, rows M2 * N1 apart.
+__host__ __device__ constexpr int spill_yt(int N1) { return N1 < 16 ? N1 : 16; }
+__host__ __device__ inline long long spill_tile_offset(int slot, int z, int yt, int N0, int N1, int M2) {
+  const int YT = spill_yt(N1);
+  return (((long long)slot * N0 + z) * (N1 / YT) + yt) * (long long)(M2 * YT);
+}
+__host__ __device__ constexpr int spill_in_tile(int kx, int yy, int YT) { return kx * YT + (yy ^ (kx & (YT - 1))); }
+__host__ __device__ inline long long spill_index(int slot, int z, int kx, int y, int N0, int N1, int M2) {
+  const int YT = spill_yt(N1);
+  return spill_tile_offset(slot, z, y / YT, N0, N1, M2) + spill_in_tile(kx, y % YT, YT);
+}
+
+// Rows of one (slot, kx) plane of the spill, for pass B (N1 a compile-time constant).
+template <int N1>
+struct SpillPlane {
+  static constexpr int YT = spill_yt(N1);
+  float2* base;    // element (z, y) at base + z * rs + (y / YT) * cs + ((y % YT) ^ sw)
+  long long rs;    // z pitch: M2 * N1
+  long long cs;    // y-chunk pitch: M2 * YT
+  int sw;          // kx % YT
+  __device__ __forceinline__ SpillPlane(float2* spill, int slot, int kx, int N0, int M2) {
+    base = spill + spill_tile_offset(slot, 0, 0, N0, N1, M2) + (long long)kx * YT;
+    rs = (long long)M2 * N1;
+    cs = (long long)M2 * YT;
+    sw = kx & (YT - 1);
+  }
+  __device__ __forceinline__ long long off(int z, int y) const {
+    return z * rs + (long long)(y / YT) * cs + ((y % YT) ^ sw);
+  }
+  __device__ __forceinline__ float2& at(int z, int y) const { return base[off(z, y)]; }
+};
+
 // ---------------------------------------------------------------- launch geometry ----
-// Pass A / C: a CTA covers YT consecutive y lines of one z plane of one system and loops
-// over the system's coils; every team of S lanes transforms LPT of the lines.
+// Pass A / C: a CTA covers YT consecutive y lines (one spill y-tile) of one z plane of one
+// system and loops over the system's coils; every team of S lanes transforms LPT lines.
 template <int N2, int YT>
 struct XPassCfg {
   static constexpr int M2 = 2 * N2;
@@ -37,17 +79,20 @@ struct XPassCfg {
   static constexpr int LPT = (YT * S > 256) ? (YT * S / 256) : 1;
   static constexpr int THREADS = YT * S / LPT;
   static constexpr int NTEAMS = THREADS / S;
-  static constexpr int TILE_LD = YT + 1;  // padded row of the [kx][y] tile
   static constexpr int TBUF = team_buf_stride<M2>();
-  // a [kx][y] tile; the same space serves as the teams' FFT exchange buffers
-  static constexpr int TILE = (M2 * TILE_LD > NTEAMS * TBUF) ? M2 * TILE_LD : NTEAMS * TBUF;
+  static constexpr int TILE_ELEMS = M2 * YT;           // one spill tile, dense (swizzled)
+  static constexpr unsigned TILE_BYTES = TILE_ELEMS * 8u;
+  // pass A: the tile; the same space serves as the teams' FFT exchange buffers
+  static constexpr int TILE = (TILE_ELEMS > NTEAMS * TBUF) ? TILE_ELEMS : NTEAMS * TBUF;
   static constexpr int SMT = YT * N2;     // one coil's map rows [y][x]
-  // float2 slots of dynamic shared memory: pass A = one tile (also the exchange
-  // buffers) + two coil-map stages; pass C = two tiles + the exchange buffers; each
-  // + the M2-entry twiddle table
+  // float2 slots of dynamic shared memory: pass A = one tile (also the exchange buffers)
+  // + two coil-map stages; pass C = two tiles + the exchange buffers; each + the M2-entry
+  // twiddle table
   static constexpr int SMEM_F2 = TILE + 2 * SMT + M2;
-  static constexpr int SMEM_F2_C = 2 * M2 * TILE_LD + NTEAMS * TBUF + M2;
+  static constexpr int SMEM_F2_C = 2 * TILE_ELEMS + NTEAMS * TBUF + M2;
   static_assert(THREADS % 32 == 0, "x-pass CTA must be whole warps");
+  static_assert((YT & (YT - 1)) == 0, "the tile swizzle needs a power-of-two tile height");
+  static_assert(TILE_BYTES % 16 == 0 && (SMT * 8) % 16 == 0, "bulk copies move whole 16-byte units");
 };
 
 // Row handled by team j of a row stage: the teams sharing a half-warp take rows S apart,
@@ -135,7 +180,8 @@ struct PassArgs {
   const float* const* sys_diag;    // [nsys] packed diagonal [M2][2][N1][M0]
   const float* sys_lambda;         // [nsys] adds lambda * x (nullable = 0)
   const float2* mul;               // [N0][N1][N2] unconjugated multiplier (single system, nullable)
-  float2* spill;                   // [nslots][N0][M2][N1], see spill_offset
+  float2* spill;                   // [nslots][N0][N1/YT][M2][YT], see spill_index
+  int* wait_error;                 // set to 1 when a pass gave up waiting for a bulk copy
   const float2* tables;            // twiddle tables, see table_offsets
   long long out_ldz, out_ldy;      // element strides of every output image
   int accumulate;                  // 1: out += result, 0: out = result
@@ -143,12 +189,6 @@ struct PassArgs {
   int prefetch_ahead;              // mod-4 plane pass: L2-prefetch distance in clusters (0 = off)
 };
 
-// Spill layout [slot][z][kx][y]: the [kx][y] tile of one (slot, z) that passes A and C
-// move is one contiguous M2*N1 block, and row z of the (slot, kx) plane that pass B
-// transforms is N1 contiguous values, M2*N1 apart from row z + 1.
-__host__ __device__ inline long long spill_offset(int slot, int z, int kx, int N0, int N1, int M2) {
-  return (((long long)slot * N0 + z) * M2 + kx) * N1;
-}
 
 // ------------------------------------------------------------------------ pass A ----
 // Per (system, z, y-tile): the x lines stay in registers while the coils stream by; coil
@@ -158,8 +198,8 @@ __global__ void __launch_bounds__(XPassCfg<N2, YT>::THREADS)
 expand_fwd_x_kernel(PassArgs a) {
   using C = XPassCfg<N2, YT>;
   constexpr int M2 = C::M2, E = C::E, S = C::S, LPT = C::LPT;
-  extern __shared__ float2 smem[];
-  float2* tile = smem;                // [M2][TILE_LD] output tile / exchange buffers
+  extern __shared__ __align__(128) float2 smem[];
+  float2* tile = smem;                // spill tile [M2][YT] (swizzled) / exchange buffers
   float2* smt = tile + C::TILE;       // 2 x [YT][N2] coil-map stages
   float2* tw = smt + 2 * C::SMT;      // [M2]
 
@@ -176,36 +216,81 @@ expand_fwd_x_kernel(PassArgs a) {
   const long long plane = (long long)N1 * N2;
   const float2* sm = a.sys_smaps[sys];
   const int slot0 = a.sys_slot0[sys], ncoil = a.sys_nslot[sys];
-
-  auto prefetch = [&](int ci) {  // coil ci's map rows [y0, y0 + YT) of plane z
+  // Coil ci's map rows [y0, y0 + YT) of plane z are one contiguous block: one bulk copy
+  // into smt[ci & 1], landing on bar[ci & 1] (phase ci >> 1), when the maps are 16-byte
+  // aligned; per-thread 8-byte asynchronous copies otherwise.
+  __shared__ __align__(8) uint64_t bar[3];  // [0], [1]: map stages; [2]: the image rows
+  __shared__ int abort_sh;
+  const bool bulk_maps = sm && (((uintptr_t)sm) & 15u) == 0;
+  const float2* xs = a.sys_x[sys] + (long long)z * plane + (long long)y0 * N2;  // rows [y0, y0 + YT)
+  const bool bulk_x = (((uintptr_t)xs) & 15u) == 0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 3; ++i) mbar_init(smem_u32(&bar[i]), 1);
+    fence_mbar_init();
+    abort_sh = 0;
+  }
+  __syncthreads();
+  // the image rows of this tile, once: one bulk copy into the second map stage, which the
+  // first map copy into it (coil 1) waits for below
+  if (bulk_x && threadIdx.x == 0) {
+    mbar_expect_tx(smem_u32(&bar[2]), C::SMT * 8u);
+    bulk_copy_g2s(smem_u32(smt + C::SMT), xs, C::SMT * 8u, smem_u32(&bar[2]));
+  }
+  int issued = 0, landed = 0;  // map copies issued (thread 0) / waited for
+  auto prefetch = [&](int ci) {
     const float2* src = sm + ((long long)a.slot_coil[slot0 + ci] * N0 + z) * plane + (long long)y0 * N2;
     float2* dst = smt + (ci & 1) * C::SMT;
-    for (int i = threadIdx.x; i < C::SMT; i += C::THREADS) cp_async8(dst + i, src + i);
-    cp_async_commit();
+    if (bulk_maps) {
+      if (threadIdx.x == 0) {
+        const uint32_t b = smem_u32(&bar[ci & 1]);
+        mbar_expect_tx(b, C::SMT * 8u);
+        bulk_copy_g2s(smem_u32(dst), src, C::SMT * 8u, b);
+        issued = ci + 1;
+      }
+    } else {
+      for (int i = threadIdx.x; i < C::SMT; i += C::THREADS) cp_async8(dst + i, src + i);
+      cp_async_commit();
+    }
   };
   if (sm && ncoil > 0) prefetch(0);
 
+  // the x lines stay in registers while the coils stream by
   float2 xv[LPT][E / 2];
+  bool x_ok = true;
+  if (bulk_x) x_ok = mbar_wait(smem_u32(&bar[2]), 0, &abort_sh);
   {
-    const float2* xs = a.sys_x[sys] + (long long)z * plane;
+    const float2* xsrc = bulk_x ? smt + C::SMT : xs;
 #pragma unroll
     for (int l = 0; l < LPT; ++l)
 #pragma unroll
-      for (int e = 0; e < E / 2; ++e)
-        xv[l][e] = xs[(long long)(y0 + team + l * C::NTEAMS) * N2 + din_index<M2>(t, e)];
+      for (int e = 0; e < E / 2; ++e) xv[l][e] = xsrc[(team + l * C::NTEAMS) * N2 + din_index<M2>(t, e)];
+  }
+  if (!x_ok) abort_sh = 1;
+  __syncthreads();  // every thread has its x lines: the second map stage may be refilled
+  if (abort_sh && bulk_x && threadIdx.x == 0) {
+    const long long t0 = clock64();  // drain the image copy (bounded) before anything else
+    while (!mbar_try_wait(smem_u32(&bar[2]), 0) && clock64() - t0 < kWaitCycles) {
+    }
   }
 
 #pragma unroll 1
   for (int ci = 0; ci < ncoil; ++ci) {
     if (sm) {
-      if (ci + 1 < ncoil) {
-        prefetch(ci + 1);
+      if (ci + 1 < ncoil) prefetch(ci + 1);
+      if (bulk_maps) {
+        if (!mbar_wait(smem_u32(&bar[ci & 1]), (ci >> 1) & 1, &abort_sh)) abort_sh = 1;
+      } else if (ci + 1 < ncoil) {
         cp_async_wait<1>();  // coil ci's rows have landed
       } else {
         cp_async_wait<0>();
       }
     }
-    __syncthreads();  // coil ci's rows are visible; the previous tile has been stored
+    // the previous coil's tile has been read out by its bulk store: the space may take
+    // this coil's exchanges
+    if (threadIdx.x == 0 && ci > 0) bulk_wait_read0();
+    __syncthreads();  // coil ci's rows are visible; the tile space is free
+    if (abort_sh) break;  // read after the barrier: the same decision in every thread
+    landed = ci + 1;
     const float2* mt = smt + (ci & 1) * C::SMT;
     float2 v[LPT][E];
 #pragma unroll
@@ -221,25 +306,55 @@ expand_fwd_x_kernel(PassArgs a) {
     for (int l = 0; l < LPT; ++l) {
       const int line = team + l * C::NTEAMS;
 #pragma unroll
-      for (int r = 0; r < E; ++r) tile[dout_index<M2>(t, r) * C::TILE_LD + line] = v[l][r];
+      for (int r = 0; r < E; ++r) tile[spill_in_tile(dout_index<M2>(t, r), line, YT)] = v[l][r];
     }
+    fence_proxy_async_smem();  // the tile's writes become visible to the bulk copy
     __syncthreads();
-    float2* dst = a.spill + spill_offset(slot0 + ci, z, 0, N0, N1, M2) + y0;
-    for (int i = threadIdx.x; i < M2 * YT; i += C::THREADS) {
-      const int kx = i / YT, j = i % YT;
-      dst[kx * N1 + j] = tile[kx * C::TILE_LD + j];
+    if (threadIdx.x == 0) {
+      bulk_copy_s2g(a.spill + spill_tile_offset(slot0 + ci, z, blockIdx.x, N0, N1, M2), smem_u32(tile),
+                    C::TILE_BYTES);
+      bulk_commit();
+    }
+  }
+  if (threadIdx.x == 0) {
+    bulk_wait0();  // the tiles are in global memory before the CTA ends
+    if (abort_sh) {
+      // a map copy did not land in time: wait (bounded, one by one) for the copies still
+      // in flight so none writes into shared memory after the CTA ends, and report
+      for (int j = landed; j < issued; ++j) {
+        const long long t0 = clock64();
+        while (!mbar_try_wait(smem_u32(&bar[j & 1]), (j >> 1) & 1) && clock64() - t0 < kWaitCycles) {
+        }
+      }
+      if (a.wait_error) atomicExch(a.wait_error, 1);
     }
   }
 }
 
-// L2 prefetch (a hint) of rows [r0, r0 + nrows) of a spill plane, rows `pitch` apart,
-// N1 values each, in 128-byte lines spread over the CTA's threads
-template <int THREADS>
-__device__ __forceinline__ void prefetch_plane_rows_l2(const float2* plane, long long pitch, int r0, int nrows,
-                                                       int N1) {
-  const int lines = N1 * (int)sizeof(float2) / 128;  // per row
-  for (int i = threadIdx.x; i < nrows * lines; i += THREADS) {
-    const char* p = (const char*)(plane + (long long)(r0 + i / lines) * pitch) + (i % lines) * 128;
+// Lane t's EZ diagonal values of one z column: the packed column stores them contiguously
+// at t*EZ (diag_pack_kernel), read as 16-byte vectors (EZ is a multiple of 4).
+template <int EZ>
+__device__ __forceinline__ void load_tcol(float* dst, const float* col, int t) {
+  static_assert(EZ % 4 == 0, "whole 16-byte vectors");
+  const float4* src = reinterpret_cast<const float4*>(col + t * EZ);
+#pragma unroll
+  for (int j = 0; j < EZ / 4; ++j) {
+    const float4 v = __ldg(src + j);
+    dst[4 * j] = v.x;
+    dst[4 * j + 1] = v.y;
+    dst[4 * j + 2] = v.z;
+    dst[4 * j + 3] = v.w;
+  }
+}
+
+// L2 prefetch (a hint) of rows [r0, r0 + nrows) of a spill plane: each row is N1 / YT
+// chunks of YT values (YT * 8 bytes, at least 64), one prefetch per chunk, spread over the
+// CTA's threads
+template <int THREADS, int N1>
+__device__ __forceinline__ void prefetch_plane_rows_l2(const SpillPlane<N1>& pl, int r0, int nrows) {
+  constexpr int YT = SpillPlane<N1>::YT, CH = N1 / YT;
+  for (int i = threadIdx.x; i < nrows * CH; i += THREADS) {
+    const float2* p = pl.base + (r0 + i / CH) * pl.rs + (long long)(i % CH) * pl.cs;
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
   }
 }
@@ -265,7 +380,6 @@ plane_yz_kernel(PassArgs a) {
   const int h = rank / Q;  // ky parity
   const int q = rank % Q;  // owned column / row block
   const int M2 = 2 * a.N2;
-  const long long RS = (long long)M2 * N1;  // spill row pitch of a plane
 
   const TableOffsets to = table_offsets(N0, N1, a.N2);
   for (int i = threadIdx.x; i < N1; i += C::THREADS) {
@@ -290,7 +404,7 @@ plane_yz_kernel(PassArgs a) {
     const int kx = (int)(item / a.nslots);
     const int sys = a.slot_sys[slot];
     if (a.active && !a.active[sys]) continue;  // uniform for the whole cluster
-    float2* g = a.spill + spill_offset(slot, 0, kx, N0, N1, M2);  // row z at g + z * RS
+    const SpillPlane<N1> g(a.spill, slot, kx, N0, M2);  // element (z, y) at g.at(z, y)
     const float* T = a.sys_diag[sys] + (((long long)kx * 2 + h) * N1) * M0;
 
     // Q == 1: the plane lands in the (row-major, padded) column buffer in row groups of
@@ -303,15 +417,15 @@ plane_yz_kernel(PassArgs a) {
       for (int grp = 0; grp < NGRP; ++grp) {
         const int r0 = grp * RG, nr = (N0 - r0) < RG ? (N0 - r0) : RG;
         for (int i = threadIdx.x; i < nr * N1; i += C::THREADS)
-          cp_async8(&P[(r0 + i / N1) * LDP + (i % N1)], g + (long long)(r0 + i / N1) * RS + (i % N1));
+          cp_async8(&P[(r0 + i / N1) * LDP + (i % N1)], &g.at(r0 + i / N1, i % N1));
         cp_async_commit();
       }
     }
     // warm L2 with this cluster's next plane (a hint only)
     if (item + ncl < nitems) {
       const long long nx = item + ncl;
-      const float2* nxt = a.spill + spill_offset((int)(nx % a.nslots), 0, (int)(nx / a.nslots), N0, N1, M2);
-      prefetch_plane_rows_l2<C::THREADS>(nxt, RS, rank * (N0 / (2 * Q)), N0 / (2 * Q), N1);
+      const SpillPlane<N1> nxt(a.spill, (int)(nx % a.nslots), (int)(nx / a.nslots), N0, M2);
+      prefetch_plane_rows_l2<C::THREADS>(nxt, rank * (N0 / (2 * Q)), N0 / (2 * Q));
     }
     // stage 1: owned rows, forward N1-point FFT of the parity-h half; each output column
     // goes to the CTA that owns it
@@ -331,7 +445,7 @@ plane_yz_kernel(PassArgs a) {
   #pragma unroll
         for (int e = 0; e < ER; ++e) {
           const int y = din_index<N1>(t, e);
-          float2 val = Q == 1 ? P[z * LDP + y] : g[(long long)z * RS + y];
+          float2 val = Q == 1 ? P[z * LDP + y] : g.at(z, y);
           if (h) val = cmul(val, par[y]);
           v[e] = val;
         }
@@ -359,9 +473,7 @@ plane_yz_kernel(PassArgs a) {
       float tnext[EZ];
       {
         const int col = team < H ? team : 0;
-        const float* Tc = T + (long long)(q * H + col) * M0;
-  #pragma unroll
-        for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tc + dout_index<M0>(t, r));
+        load_tcol<EZ>(tnext, T + (long long)(q * H + col) * M0, t);
       }
   #pragma unroll 1
       for (int c0 = 0; c0 < H; c0 += C::NTEAMS_Z) {
@@ -373,9 +485,7 @@ plane_yz_kernel(PassArgs a) {
         for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
         if (c0 + C::NTEAMS_Z < H) {
           const int cn = c0 + C::NTEAMS_Z + team;
-          const float* Tn = T + (long long)(q * H + (cn < H ? cn : 0)) * M0;
-  #pragma unroll
-          for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tn + dout_index<M0>(t, r));
+          load_tcol<EZ>(tnext, T + (long long)(q * H + (cn < H ? cn : 0)) * M0, t);
         }
         float2 v[EZ];
   #pragma unroll
@@ -429,7 +539,7 @@ plane_yz_kernel(PassArgs a) {
       constexpr int HALF = ZR / 2;
       for (int i = threadIdx.x; i < HALF * N1; i += C::THREADS) {
         const int zl = h * HALF + i / N1, y = i % N1;
-        g[(long long)(q * ZR + zl) * RS + y] = cadd(P[zl * GROW + y], other[zl * GROW + y]);
+        g.at(q * ZR + zl, y) = cadd(P[zl * GROW + y], other[zl * GROW + y]);
       }
     }
 
@@ -516,14 +626,13 @@ plane_mod_kernel(PassArgs a) {
   for (int i = threadIdx.x; i < M1; i += C::THREADS) circ[i] = a.tables[to.circ + i];
   __syncthreads();
 
-  const long long RS = (long long)M2 * N1;  // spill row pitch of a plane
-  float2* g = a.spill + spill_offset(slot, 0, kx, N0, N1, M2);  // row z at g + z * RS
+  const SpillPlane<N1> g(a.spill, slot, kx, N0, M2);  // element (z, y) at g.at(z, y)
   {
     // warm L2 with the plane of the cluster a.prefetch_ahead clusters later (a hint only)
     const long long cl = (long long)blockIdx.z * gridDim.y + blockIdx.y + a.prefetch_ahead;
     if (a.prefetch_ahead > 0 && cl < (long long)gridDim.y * gridDim.z) {
-      const float2* nxt = a.spill + spill_offset((int)(cl % gridDim.y), 0, (int)(cl / gridDim.y), N0, N1, M2);
-      prefetch_plane_rows_l2<C::THREADS>(nxt, RS, q * (N0 / K), N0 / K, N1);
+      const SpillPlane<N1> nxt(a.spill, (int)(cl % gridDim.y), (int)(cl / gridDim.y), N0, M2);
+      prefetch_plane_rows_l2<C::THREADS>(nxt, q * (N0 / K), N0 / K);
     }
   }
   // T column of ky = K*k + q: packed index h = q & 1, ky' = (K/2)*k + (q >> 1)
@@ -544,11 +653,11 @@ plane_mod_kernel(PassArgs a) {
     for (int e = 0; e < ER; ++e) cw[e] = circ[(din_index<L>(t, e) * q) % M1];
     float2 nv[NM][ER];  // the next row's values, loaded while the current one is transformed
     {
-      const float2* row = g + (long long)(tr < N0 ? tr : 0) * RS;
+      const int z0 = tr < N0 ? tr : 0;
 #pragma unroll
       for (int m = 0; m < NM; ++m)
 #pragma unroll
-        for (int e = 0; e < ER; ++e) nv[m][e] = row[din_index<L>(t, e) + L * m];
+        for (int e = 0; e < ER; ++e) nv[m][e] = g.at(z0, din_index<L>(t, e) + L * m);
     }
 #pragma unroll 1
     for (int it = 0; it < C::LPT; ++it) {
@@ -562,12 +671,11 @@ plane_mod_kernel(PassArgs a) {
         v[e] = q == 0 ? acc : cmul(acc, cw[e]);
       }
       if (it + 1 < C::LPT) {
-        const int zn = z + C::NTEAMS_R;
-        const float2* row = g + (long long)(zn < N0 ? zn : 0) * RS;
+        const int zn = z + C::NTEAMS_R < N0 ? z + C::NTEAMS_R : 0;
 #pragma unroll
         for (int m = 0; m < NM; ++m)
 #pragma unroll
-          for (int e = 0; e < ER; ++e) nv[m][e] = row[din_index<L>(t, e) + L * m];
+          for (int e = 0; e < ER; ++e) nv[m][e] = g.at(zn, din_index<L>(t, e) + L * m);
       }
       team_fft_din_to_dout_r<L, -1, false>(v, t, buf, twr);
       if (z < N0) {
@@ -588,11 +696,7 @@ plane_mod_kernel(PassArgs a) {
     if constexpr (kRegTw) load_lane_twiddles<M0>(twz, tw_z, t);
     auto tcol = [&](int col) { return T + (long long)((K / 2) * col + (q >> 1)) * M0; };
     float tnext[EZ];
-    {
-      const float* Tc = tcol(team < L ? team : 0);
-#pragma unroll
-      for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tc + dout_index<M0>(t, r));
-    }
+    load_tcol<EZ>(tnext, tcol(team < L ? team : 0), t);
 #pragma unroll 1
     for (int c0 = 0; c0 < L; c0 += C::NTEAMS_Z) {
       const int col = c0 + team;
@@ -603,9 +707,7 @@ plane_mod_kernel(PassArgs a) {
       for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
       if (c0 + C::NTEAMS_Z < L) {
         const int cn = c0 + C::NTEAMS_Z + team;
-        const float* Tn = tcol(cn < L ? cn : 0);
-#pragma unroll
-        for (int r = 0; r < EZ; ++r) tnext[r] = __ldg(Tn + dout_index<M0>(t, r));
+        load_tcol<EZ>(tnext, tcol(cn < L ? cn : 0), t);
       }
       float2 v[EZ];
 #pragma unroll
@@ -667,11 +769,15 @@ plane_mod_kernel(PassArgs a) {
       for (int qq = 1; qq < K; ++qq) u[qq] = cmulc(R[qq][z * LDP + y], cy[qq]);
       Dft<K, 1>::run(u);
 #pragma unroll
-      for (int m = 0; m < NM; ++m) g[(long long)z * RS + y + L * m] = u[m];
+      for (int m = 0; m < NM; ++m) g.at(z, y + L * m) = u[m];
     }
   }
-  // keep this CTA's shared memory alive until the partners have read it
-  cluster.sync();
+  // Keep this CTA's shared memory alive until the partners have read it.  Every value a
+  // thread read from a partner was consumed by the stores above, so those reads have been
+  // performed; the arrive needs no release ordering (which would also wait for this CTA's
+  // global stores to complete), hence the relaxed form.
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
 }
 
 // ------------------------------------------------------------------------ pass C ----
@@ -680,11 +786,13 @@ __global__ void __launch_bounds__(XPassCfg<N2, YT>::THREADS)
 inv_x_combine_kernel(PassArgs a) {
   using C = XPassCfg<N2, YT>;
   constexpr int M2 = C::M2, E = C::E, S = C::S, LPT = C::LPT;
-  extern __shared__ float2 smem[];
-  float2* tiles = smem;                          // 2 x [M2][TILE_LD]
-  float2* xbuf = tiles + 2 * M2 * C::TILE_LD;    // teams' exchange buffers
+  extern __shared__ __align__(128) float2 smem[];
+  float2* tiles = smem;                          // 2 x spill tile [M2][YT] (swizzled)
+  float2* xbuf = tiles + 2 * C::TILE_ELEMS;      // teams' exchange buffers
   float2* tw = xbuf + C::NTEAMS * C::TBUF;
   __shared__ double red[32];
+  __shared__ __align__(8) uint64_t bar[2];       // tile ci landed: bar[ci & 1], phase ci >> 1
+  __shared__ int abort_sh;
 
   const int sys = blockIdx.z;
   if (a.active && !a.active[sys]) return;
@@ -692,22 +800,26 @@ inv_x_combine_kernel(PassArgs a) {
   const int y0 = blockIdx.x * YT;
   const int N0 = a.N0, N1 = a.N1;
 
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bar[0]), 1);
+    mbar_init(smem_u32(&bar[1]), 1);
+    fence_mbar_init();
+    abort_sh = 0;
+  }
   for (int i = threadIdx.x; i < M2; i += C::THREADS) tw[i] = a.tables[i];
+  __syncthreads();
 
   const int team = threadIdx.x / S, t = threadIdx.x % S;
   float2* buf = xbuf + team * C::TBUF;
   const long long plane = (long long)N1 * N2;
 
   const int slot0 = a.sys_slot0[sys], ncoil = a.sys_nslot[sys];
-  // asynchronous copy of coil ci's [kx][y] tile into tiles[ci & 1]
-  auto prefetch = [&](int ci) {
-    const float2* src = a.spill + spill_offset(slot0 + ci, z, 0, N0, N1, M2) + y0;
-    float2* dst = tiles + (ci & 1) * M2 * C::TILE_LD;
-    for (int i = threadIdx.x; i < M2 * YT; i += C::THREADS) {
-      const int kx = i / YT, j = i % YT;
-      cp_async8(&dst[kx * C::TILE_LD + j], src + kx * N1 + j);
-    }
-    cp_async_commit();
+  // one bulk copy of coil ci's spill tile into tiles[ci & 1] (thread 0)
+  auto issue = [&](int ci) {
+    const uint32_t b = smem_u32(&bar[ci & 1]);
+    mbar_expect_tx(b, C::TILE_BYTES);
+    bulk_copy_g2s(smem_u32(tiles + (ci & 1) * C::TILE_ELEMS),
+                  a.spill + spill_tile_offset(slot0 + ci, z, blockIdx.x, N0, N1, M2), C::TILE_BYTES, b);
   };
 
   float2 acc[LPT][E / 2];
@@ -717,19 +829,23 @@ inv_x_combine_kernel(PassArgs a) {
     for (int e = 0; e < E / 2; ++e) acc[l][e] = make_float2(0.f, 0.f);
 
   const float2* sm = a.sys_smaps[sys];
-  if (ncoil > 0) prefetch(0);
+  if (threadIdx.x == 0 && ncoil > 0) issue(0);
+  int issued = ncoil > 0 ? 1 : 0;  // thread 0's count of copies issued
+  int landed = 0;                  // copies whose wait completed
 #pragma unroll 1
   for (int ci = 0; ci < ncoil; ++ci) {
-    if (ci + 1 < ncoil) {
-      prefetch(ci + 1);
-      cp_async_wait<1>();  // coil ci's tile has landed
-    } else {
-      cp_async_wait<0>();
+    // the buffer of coil ci + 1 was released by the barrier at the end of coil ci - 1
+    if (threadIdx.x == 0 && ci + 1 < ncoil) {
+      issue(ci + 1);
+      issued = ci + 2;
     }
+    if (!mbar_wait(smem_u32(&bar[ci & 1]), (ci >> 1) & 1, &abort_sh)) abort_sh = 1;
     __syncthreads();
+    if (abort_sh) break;  // read after the barrier: the same decision in every thread
+    landed = ci + 1;
     const int coil = a.slot_coil[slot0 + ci];
     const float2* ss = sm ? sm + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
-    const float2* tile = tiles + (ci & 1) * M2 * C::TILE_LD;
+    const float2* tile = tiles + (ci & 1) * C::TILE_ELEMS;
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
       const int line = team + l * C::NTEAMS;
@@ -743,7 +859,7 @@ inv_x_combine_kernel(PassArgs a) {
       }
       float2 v[E];
 #pragma unroll
-      for (int r = 0; r < E; ++r) v[r] = tile[dout_index<M2>(t, r) * C::TILE_LD + line];
+      for (int r = 0; r < E; ++r) v[r] = tile[spill_in_tile(dout_index<M2>(t, r), line, YT)];
       team_fft_dout_to_din<M2, 1, true>(v, t, buf, tw);
 #pragma unroll
       for (int e = 0; e < E / 2; ++e) {
@@ -752,6 +868,19 @@ inv_x_combine_kernel(PassArgs a) {
       }
     }
     __syncthreads();  // this tile buffer is refilled two coils later
+  }
+  if (abort_sh) {
+    // a copy did not land in time: wait (bounded, one by one) for the copies still in
+    // flight so none writes into shared memory after the CTA ends, report, write nothing
+    if (threadIdx.x == 0) {
+      for (int j = landed; j < issued; ++j) {
+        const long long t0 = clock64();
+        while (!mbar_try_wait(smem_u32(&bar[j & 1]), (j >> 1) & 1) && clock64() - t0 < kWaitCycles) {
+        }
+      }
+      if (a.wait_error) atomicExch(a.wait_error, 1);
+    }
+    return;
   }
 
   // epilogue

@@ -75,9 +75,20 @@ class BatchedSenseNormalToeplitz:
         BF16 hi + lo operands and FP32 accumulation (ny = nx = 128)."""
         self._senseop.set_precision(precision)
 
-    def cg(self, x, b, iters=30, tol=0.0, lamda=0.0, coils=None):
-        """ConjugateGradient on (A^H A)_toeplitz + lamda I for every outer batch of x (in place)."""
-        return self._senseop.cg(x, b, int(iters), float(tol), float(lamda), coils)
+    def cg(self, x, b, iters=30, tol=0.0, lamda=0.0, coils=None, precond=None, centered=True):
+        """ConjugateGradient on (A^H A)_toeplitz + lamda I for every outer batch of x (in
+        place).  With ``precond`` (a circulant preconditioner diagonal, centred as
+        ``circulant_precond_diagonal`` returns it unless ``centered=False``) the solve is
+        preconditioned CG with CirculantPreconditionerOp(precond, centered)."""
+        if precond is None:
+            return self._senseop.cg(x, b, int(iters), float(tol), float(lamda), coils)
+        return self._senseop.pcg(x, b, int(iters), float(tol), float(lamda), coils, precond, bool(centered))
+
+
+def circulant_precond_diagonal(smaps, coord, lamda=0.0):
+    """CirculantPreconditionerOp::build_diagonal (precond.cpp:65-117): the centred inverse
+    Fourier-domain diagonal of the SENSE normal operator plus lamda, float32 [nz, ny, nx]."""
+    return torch.ops.HastyToeplitz.circulant_precond_diagonal(smaps, coord, float(lamda))
 
 
 def batched_sense_toeplitz_diagonals(input, coil_list, smaps, diagonals, streams=None):

@@ -114,7 +114,19 @@ class AdmissionQueue:
 
 
 class ReconServer:
-    def __init__(self, device=None, hbm_budget_bytes=None, max_active=4, graph=True, precision="fp32"):
+    """Served reconstruction loop.
+
+    mode "batching" (default): continuous batching.  Each image size has one running batch
+    of CG solves on the device (``CgBatch``) with a fixed share of the HBM budget; every
+    frame x encoding system of an arriving job waits in that size's queue and joins the
+    batch at the next iteration boundary at which its memory fits (admission by HBM
+    footprint), so the systems of all jobs in flight advance together, one launch sequence
+    per iteration, and leave as they finish.  A job is done when its last system leaves.
+    mode "streams": each admitted job solves its systems alone on its own CUDA stream
+    (kernels of concurrent jobs overlap only as the GPU's scheduler allows)."""
+
+    def __init__(self, device=None, hbm_budget_bytes=None, max_active=4, graph=True, precision="fp32",
+                 mode="batching", sizes=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if hbm_budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
@@ -133,8 +145,18 @@ class ReconServer:
         self._results = []
         self._threads = []
         self._errors = []
-        self._sched = threading.Thread(target=self._schedule, daemon=True)
-        self._sched.start()
+        if mode not in ("batching", "streams"):
+            raise ValueError(f"mode must be 'batching' or 'streams', got {mode!r}")
+        self.mode = mode
+        self._workers = {}
+        self._sizes = [tuple(int(n) for n in sz) for sz in (sizes or [])]
+        if mode == "batching":
+            self._sched = None
+            for sz in self._sizes:  # workers for the sizes known up front (more on first use)
+                self._worker(sz)
+        else:
+            self._sched = threading.Thread(target=self._schedule, daemon=True)
+            self._sched.start()
 
     # ------------------------------------------------------------------ public ----
     def submit(self, job: ReconJob) -> Future:
@@ -144,6 +166,10 @@ class ReconServer:
                 raise RuntimeError("server is closed")
             job.job_id = self._next_id if job.job_id < 0 else job.job_id
             self._next_id += 1
+            if self.mode == "batching":
+                self._worker(tuple(int(n) for n in job.shape)).enqueue(job, fut, time.perf_counter())
+                self._cv.notify_all()
+                return fut
             fp = job_footprint(job, self._plan(job.shape))
             try:
                 self._queue.push((job, fut, time.perf_counter()), fp)
@@ -157,9 +183,12 @@ class ReconServer:
             self._closed = True
             self._cv.notify_all()
         if wait:
-            self._sched.join()
+            if self._sched is not None:
+                self._sched.join()
             for t in list(self._threads):
                 t.join()
+            for w in list(self._workers.values()):
+                w.thread.join()
         if self._errors:
             raise self._errors[0]
 
@@ -182,6 +211,15 @@ class ReconServer:
         if shape not in self._plans:
             self._plans[shape] = ToeplitzPlan(shape, self.device)
         return self._plans[shape]
+
+    def _worker(self, shape):
+        """The running batch of one image size (created under self._cv or at start-up)."""
+        w = self._workers.get(shape)
+        if w is None:
+            w = _SizeWorker(self, shape)
+            self._workers[shape] = w
+            w.thread.start()
+        return w
 
     def _schedule(self):
         while True:
@@ -227,3 +265,112 @@ class ReconServer:
             with self._cv:
                 self._queue.release(fp)
                 self._cv.notify_all()
+
+
+class _JobState:
+    def __init__(self, job, fut, t_submit, device):
+        self.job, self.fut, self.t_submit = job, fut, t_submit
+        nsys = len(job.frame_of_system)
+        self.x = torch.zeros((nsys,) + tuple(job.shape), dtype=torch.complex64, device=device)
+        self.status = [0] * nsys
+        self.iters = [0] * nsys
+        self.remaining = nsys
+        self.t_admit = None
+
+
+class _SizeWorker:
+    """One image size of the batching server: a CgBatch fed from a FIFO of systems."""
+
+    def __init__(self, server, shape):
+        self.server = server
+        self.shape = shape
+        dev = server.device
+        self.plan = ToeplitzPlan(shape, dev)
+        if server.precision != "fp32" and shape[1:] == (128, 128):
+            self.plan.set_precision(server.precision)
+        # capacity: an equal share of the budget for each size named at start-up, half of
+        # what is left for a size that was not (at least one 32-coil system); per
+        # (system, coil) slot the spill of 2 images, per system r, p, Ap
+        nv = 1
+        for n in shape:
+            nv *= int(n)
+        if shape in server._sizes:
+            share = server.budget // len(server._sizes)
+        else:
+            server._unlisted_left = getattr(server, "_unlisted_left", server.budget)
+            share = server._unlisted_left // 2
+            server._unlisted_left -= share
+        per_slot = 16 * nv
+        max_slots = int(max(32, min(65535, share // (per_slot + 3 * 8 * nv // 8))))
+        max_sys = int(max(1, min(4096, max_slots // 4)))
+        while max_slots > 32:
+            nb = int(self.plan.lib.hb_cg_batch_workspace_bytes(self.plan._h, max_sys, max_slots))
+            if nb <= share:
+                break
+            max_slots = int(max_slots * 0.9)
+            max_sys = int(max(1, min(max_sys, max_slots // 4)))
+        self.batch = self.plan.cg_batch(max_sys, max_slots)
+        self.queue = collections.deque()   # (job state, system index), arrival order
+        self.owner = {}                    # handle -> (job state, system index)
+        self.thread = threading.Thread(target=self._loop, daemon=True)
+
+    def enqueue(self, job, fut, t_submit):
+        js = _JobState(job, fut, t_submit, self.server.device)
+        for s in range(len(job.frame_of_system)):
+            self.queue.append((js, s))
+
+    def _admit(self):
+        """Adds queued systems in arrival order while the batch has room (no overtaking)."""
+        from . import capi
+
+        while True:
+            with self.server._cv:
+                if not self.queue:
+                    return
+                js, s = self.queue[0]
+            job = js.job
+            q = System(js.x[s], job.smaps, job.packed_diags[job.frame_of_system[s]], b=job.b[s], coils=job.coils,
+                       lam=job.lam)
+            try:
+                h = self.batch.add(q, job.iters, job.tol)
+            except capi.HastyError as e:
+                if e.code == capi.HB_ERR_WORKSPACE:
+                    return  # full: retry at the next iteration boundary
+                raise
+            with self.server._cv:
+                self.queue.popleft()
+            self.owner[h] = (js, s)
+            if js.t_admit is None:
+                js.t_admit = time.perf_counter()
+
+    def _loop(self):
+        srv = self.server
+        try:
+            torch.cuda.set_device(srv.device)
+            stream = torch.cuda.Stream(srv.device)
+            with torch.cuda.stream(stream):
+                while True:
+                    with srv._cv:
+                        while not self.queue and not self.owner and not srv._closed:
+                            srv._cv.wait()
+                        if srv._closed and not self.queue and not self.owner:
+                            return
+                    self._admit()
+                    self.batch.step(stream)
+                    for h, st, it in self.batch.retire():
+                        js, s = self.owner.pop(h)
+                        js.status[s], js.iters[s] = st, it
+                        js.remaining -= 1
+                        if js.remaining == 0:
+                            res = ReconResult(js.job.job_id, js.x, js.status, js.iters, js.t_submit, js.t_admit,
+                                              time.perf_counter())
+                            with srv._cv:
+                                srv._results.append(res)
+                            js.fut.set_result(res)
+        except Exception as e:  # reported through the futures and close()
+            with srv._cv:
+                srv._errors.append(e)
+                pending = [js for js, _ in self.owner.values()] + [js for js, _ in self.queue]
+            for js in pending:
+                if not js.fut.done():
+                    js.fut.set_exception(e)

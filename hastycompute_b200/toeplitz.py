@@ -121,6 +121,10 @@ class ToeplitzPlan:
             self._ws = torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
         return self._ws
 
+    def cg_batch(self, max_systems, max_coil_slots):
+        """A running batch of CG solves on this plan (continuous batching); see CgBatch."""
+        return CgBatch(self, max_systems, max_coil_slots)
+
     def plane_schedule(self):
         """Name of the plane-pass schedule the next call launches (``hb_plan_plane_schedule``)."""
         return self.lib.hb_plan_plane_schedule(self._h).decode()
@@ -442,3 +446,67 @@ class ToeplitzPlan:
             return list(status), list(done)
         capi.check(code)
         return list(status), list(done)
+
+
+class CgBatch:
+    """A running batch of CG solves on one plan (``hb_cg_batch_*``): systems join at the
+    next iteration boundary (``add``), every ``step`` runs one launch sequence in which the
+    new systems initialise and every other member takes one CG iteration, and systems
+    leave when they converge, break down or have run their own iteration budget
+    (``retire``).  A member's iterates are bitwise those of ``ToeplitzPlan.cg_systems`` on
+    the same system, whatever else is in the batch.
+
+    Replaces the reference's thread-pool fan-out of independent CG solves
+    (``BatchedConjugateGradient::run``, ``lib/op/opalgs.ixx:93-121``) with continuous
+    batching on the device."""
+
+    def __init__(self, plan, max_systems, max_coil_slots):
+        self.plan = plan
+        self.lib = plan.lib
+        nb = int(self.lib.hb_cg_batch_workspace_bytes(plan._h, int(max_systems), int(max_coil_slots)))
+        self._ws = torch.empty(nb, dtype=torch.uint8, device=plan.device)
+        h = ctypes.c_void_p()
+        capi.check(self.lib.hb_cg_batch_create(ctypes.byref(h), plan._h, int(max_systems), int(max_coil_slots),
+                                               _ptr(self._ws), nb))
+        self._h = h
+        self._keep = {}  # handle -> tensors and coil arrays the device reads until retirement
+        self.max_systems = int(max_systems)
+        self.max_coil_slots = int(max_coil_slots)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self.lib.hb_cg_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def add(self, system, iters, tol=0.0):
+        """Queues a System (x: initial guess in, solution out; b; coils; packed; lam).
+        Returns its handle; raises HastyError (HB_ERR_WORKSPACE) when the batch is full."""
+        arr, keep = self.plan._systems([system], cg=True)
+        hd = ctypes.c_int64(-1)
+        capi.check(self.lib.hb_cg_batch_add(self._h, arr, int(iters), float(tol), ctypes.byref(hd)))
+        self._keep[hd.value] = (system, keep)
+        return hd.value
+
+    def step(self, stream=None):
+        """One iteration boundary; returns the number of systems still in the batch."""
+        n = ctypes.c_int64(0)
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else _stream_ptr(self.plan.device)
+        capi.check(self.lib.hb_cg_batch_step(self._h, sp, ctypes.byref(n)))
+        return int(n.value)
+
+    def retire(self):
+        """Systems that left the batch since the last call: [(handle, status, iterations)]."""
+        cap = self.max_systems * 4 + 16
+        hs = (ctypes.c_int64 * cap)()
+        st = (ctypes.c_int32 * cap)()
+        it = (ctypes.c_int32 * cap)()
+        n = ctypes.c_int64(0)
+        capi.check(self.lib.hb_cg_batch_retire(self._h, hs, st, it, cap, ctypes.byref(n)))
+        out = [(int(hs[i]), int(st[i]), int(it[i])) for i in range(n.value)]
+        for hd, _, _ in out:
+            self._keep.pop(hd, None)
+        return out

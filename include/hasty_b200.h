@@ -82,11 +82,15 @@ int hb_plan_destroy(hb_plan* plan);
 int hb_plan_set_precision(hb_plan* plan, int precision);
 int hb_plan_precision(const hb_plan* plan);
 
-/* Reads and clears the device's flag for a tensor-core pass that gave up waiting on one
- * of its mbarriers (after about one second): HB_ERR_CUDA with a message if it was set
+/* Reads and clears the device's flag for a pass that gave up waiting on one of its
+ * mbarriers (after about one second): the x passes' bulk copies of spill tiles, or the
+ * tensor-core pass's operands and contractions.  HB_ERR_CUDA with a message if it was set
  * (the output of that launch is incomplete), else HB_OK.  Synchronous.  hb_cg_run and
- * hb_cg_run_systems check it themselves on plans set to HB_PRECISION_BF16X3; after the
- * asynchronous calls (normal op, Toeplitz apply) the caller checks it. */
+ * hb_cg_run_systems check it themselves; after the asynchronous calls (normal op,
+ * Toeplitz apply) the caller checks it.  The flag is one word per device: calls that run
+ * concurrently on one device (several streams or threads) share it, so one call's check
+ * may report, and clear, another's stall; a caller that needs the attribution runs such
+ * calls one after another. */
 int hb_wait_status(int device);
 
 /* Fault injection for tests of the path above (no counterpart in the reference): later
@@ -96,7 +100,9 @@ int hb_wait_status(int device);
  * (or the CG's own check) reports it.  chunk = -1 turns it off (the default). */
 int hb_plan_inject_tc_stall(hb_plan* plan, int chunk);
 
-/* Number of floats of one packed diagonal (= 8 * nz * ny * nx). */
+/* Number of floats of one packed diagonal (= 8 * nz * ny * nx).  Every packed diagonal
+ * passed to the calls below must start on a 16-byte boundary (HB_ERR_INVALID otherwise):
+ * the plane pass reads its z columns with 16-byte loads. */
 int64_t hb_diag_packed_floats(const hb_plan* plan);
 
 /* Pack a reference-layout diagonal T [2nz][2ny][2nx] complex64 into the internal
@@ -179,6 +185,39 @@ int hb_sense_normal_apply_systems(const hb_plan* plan, int64_t nsys, const hb_sy
 int hb_cg_run_systems(const hb_plan* plan, int64_t nsys, const hb_system* systems, int iters,
                       double tol, int flags, int32_t* status_host, int32_t* iters_done_host,
                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Running batch of CG solves (continuous batching) ----
+ *
+ * Replaces the reference's host-side fan-out of independent CG solves over a thread pool
+ * of stream contexts (BatchedConjugateGradient::run, lib/op/opalgs.ixx:93-121, fed by
+ * lib/mri/batch_sense.cpp:45-79) by one device-resident batch per image size that
+ * systems join and leave at iteration boundaries: every hb_cg_batch_step runs, in one
+ * launch sequence over all members, the initialisation of the systems added since the
+ * previous step (r = b - (A + lambda I) x, p = r) and one iteration of every other member
+ * (opalgs.cpp:50-96).  A member leaves when it converges (sqrt(Re<r, r>) < tol), breaks
+ * down (HB_CG_NOT_PD) or has run its own iteration budget.  A member's iterates are bitwise
+ * those of hb_cg_run_systems on the same system, whatever else is in the batch.
+ *
+ * The batch holds up to max_systems systems with up to max_coil_slots (system, coil)
+ * pairs in total, in a caller workspace of hb_cg_batch_workspace_bytes.  x (initial guess
+ * in, solution out) and b stay caller buffers and must stay alive until the system is
+ * retired.  Preconditioned systems (hb_system.precond) are refused (HB_ERR_UNSUPPORTED).
+ * hb_cg_batch_step synchronises `stream` (it reads the members' status back). */
+typedef struct hb_cg_batch hb_cg_batch;
+size_t hb_cg_batch_workspace_bytes(const hb_plan* plan, int64_t max_systems, int64_t max_coil_slots);
+int hb_cg_batch_create(hb_cg_batch** batch, const hb_plan* plan, int64_t max_systems, int64_t max_coil_slots,
+                       void* workspace, size_t workspace_bytes);
+int hb_cg_batch_destroy(hb_cg_batch* batch);
+/* Queues one system (copied, coil list included) with its iteration budget (>= 1) and
+ * tolerance; *handle identifies it.  HB_ERR_WORKSPACE when no capacity is free. */
+int hb_cg_batch_add(hb_cg_batch* batch, const hb_system* system, int iters, double tol, int64_t* handle);
+/* One iteration boundary for every member (see above); *in_batch receives the number of
+ * members still in the batch afterwards. */
+int hb_cg_batch_step(hb_cg_batch* batch, void* stream, int64_t* in_batch);
+/* Up to cap systems that left the batch, oldest first: handle, HB_CG_* status and
+ * iterations done (host arrays, each nullable); *n_out receives how many. */
+int hb_cg_batch_retire(hb_cg_batch* batch, int64_t* handles, int32_t* status, int32_t* iters, int64_t cap,
+                       int64_t* n_out);
 
 /* Workspace bytes of hb_cg_run for nsys systems handled at once. */
 size_t hb_cg_workspace_bytes(const hb_plan* plan, int64_t nsys, int64_t ncoil, int iters);

@@ -35,7 +35,8 @@ def test_admission_head_blocks_later_items():
 
 
 @pytest.mark.gpu
-def test_served_jobs_match_alone(cuda):
+@pytest.mark.parametrize("mode", ["batching", "streams"])
+def test_served_jobs_match_alone(cuda, mode):
     from hastycompute_b200.serve import ReconJob, ReconServer, job_footprint
     from hastycompute_b200.toeplitz import System, ToeplitzPlan
 
@@ -53,7 +54,9 @@ def test_served_jobs_match_alone(cuda):
                              b=b, iters=5, lam=1e-3))
     # budget: the largest job fits, two large ones do not -> queueing happens
     fps = [job_footprint(j, ToeplitzPlan(j.shape, cuda)) for j in jobs]
-    server = ReconServer(cuda, hbm_budget_bytes=max(fps) + min(fps), max_active=3)
+    # batching: each size's running batch gets half of that budget, so systems queue for it
+    server = ReconServer(cuda, hbm_budget_bytes=max(fps) + min(fps), max_active=3, mode=mode,
+                         sizes=[(16, 16, 16), (32, 32, 32)])
     futs = [server.submit(j) for j in jobs]
     results = [f.result(timeout=300) for f in futs]
     server.close()

@@ -174,3 +174,32 @@ def test_nufft_and_svt_torchscript_classes(cuda):
                        (7, 7, 7), 1.5, True)
     assert O.rel_l2(vt.numpy().astype(np.complex128), ref) < 1e-5
     hasty_svt.Random3DBlocksSVT().apply(vt, 10, [4, 4, 4], 2, False)  # runs; the corners are internal
+
+
+@pytest.mark.parametrize("centered", [True, False])
+def test_preconditioned_cg_through_torchscript_class(ffi, cuda, centered):
+    """ConjugateGradient with a CirculantPreconditionerOp through the TorchScript class runs
+    the fused device PCG and matches the oracle's FP64 PCG (opalgs.cpp:50-96 with P)."""
+    from hastycompute_b200.toeplitz import ToeplitzPlan
+
+    shape, lam, iters = (16, 16, 16), 1e-2, 8
+    rng = np.random.default_rng(9)
+    coords = rng.uniform(-np.pi, np.pi, (3, 3000)).astype(np.float32)
+    sm = synth.coil_maps(4, shape, seed=10)
+    ct, smt = torch.from_numpy(coords).to(cuda), torch.from_numpy(sm).to(cuda)
+    pc = ffi.circulant_precond_diagonal(smt, ct, lam)  # centred
+    Pfft = torch.fft.ifftshift(pc)  # FFT order: the layout hb_precond_build writes
+    P_plan = ToeplitzPlan(shape, cuda).build_preconditioner(ct, smt, lam=lam)
+    assert O.rel_l2(Pfft.to(torch.complex128), P_plan.to(torch.complex128)) < 1e-6
+    T = O.toeplitz_diagonal(coords.astype(np.float64), shape)
+    xtrue = synth.gaussian_image(shape, seed=11)
+    A = O.regularized(lambda v: O.sense_normal_toeplitz(v, sm, T), lam)
+    b = A(xtrue)
+    Pn = Pfft.cpu().numpy().astype(np.float64)
+    xo, done = O.conjugate_gradient(A, b, iters=iters, P=lambda r: O.precond_apply(Pn, r))
+    op = ffi.BatchedSenseNormalToeplitz(torch.from_numpy(T[None].astype(np.complex64)), smt, [0])
+    x = torch.zeros((1, 1) + shape, dtype=torch.complex64, device=cuda)
+    bt = torch.from_numpy(b.astype(np.complex64)).reshape((1, 1) + shape).to(cuda)
+    its = op.cg(x, bt, iters, 0.0, lam, None, pc if centered else Pfft, centered)
+    assert list(its) == [done]
+    assert O.rel_l2(_np(x[0, 0]), xo) < 1e-4
