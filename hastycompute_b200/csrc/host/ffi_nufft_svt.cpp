@@ -6,7 +6,9 @@
 #include <c10/cuda/CUDAGuard.h>
 #include <c10/cuda/CUDAStream.h>
 #include <ATen/ATen.h>
+#include <torch/csrc/jit/api/compilation_unit.h>
 #include <torch/custom_class.h>
+#include <torch/jit.h>
 #include <torch/library.h>
 
 #include <random>
@@ -91,10 +93,28 @@ class Nufft : public torch::CustomClassHolder {
   hb_nufft* _plan = nullptr;
 };
 
-// NufftNormal(coords, nmodes, forward_opts, backward_opts).apply(in, out, storage)
-// (CUDANufftNormal, nufft.cpp:785-920): out = backward(forward(in)), storage [ntransf, nfreq]
-// holds the k-space data in between.  The reference's optional `func_between` callback is
-// not supported here (the k-space manipulators are in hb_sense_normal_nufft).
+// FunctionLambda(script, entry, captures).apply(inout) (python/cpp/py_interface.cpp:6-15):
+// a TorchScript function compiled from `script`, called as entry(inout, captures).  The
+// reference passes it to NufftNormal.apply to act on the k-space data between the two
+// transforms.
+class FunctionLambda : public torch::CustomClassHolder {
+ public:
+  FunctionLambda(const std::string& script, const std::string& entry, const std::vector<at::Tensor>& captures)
+      : _cunit(torch::jit::compile(script)), _entry(entry), _captures(captures) {}
+  void apply(const std::vector<at::Tensor>& inout) const {
+    _cunit->run_method(_entry, c10::List<at::Tensor>(inout), c10::List<at::Tensor>(_captures));
+  }
+
+ private:
+  std::shared_ptr<torch::jit::CompilationUnit> _cunit;
+  std::string _entry;
+  std::vector<at::Tensor> _captures;
+};
+
+// NufftNormal(coords, nmodes, forward_opts, backward_opts).apply(in, out, storage, func_between)
+// (CUDANufftNormal, nufft.cpp:785-920; binding py_nufft.cpp:96-107): out = backward(f(forward(in))),
+// storage [ntransf, nfreq] holds the k-space data in between and f, when given, is a
+// FunctionLambda applied to it in place (the identity otherwise).
 class NufftNormal : public torch::CustomClassHolder {
  public:
   NufftNormal(const at::Tensor& coords, const std::vector<int64_t>& nmodes,
@@ -102,8 +122,10 @@ class NufftNormal : public torch::CustomClassHolder {
       : _fwd(c10::make_intrusive<Nufft>(coords, nmodes, fwd)), _bwd(c10::make_intrusive<Nufft>(coords, nmodes, bwd)) {
     if (fwd->type != 2 || bwd->type != 1) throw std::runtime_error("NufftNormal needs a type-2 forward and a type-1 backward");
   }
-  void apply(const at::Tensor& in, at::Tensor out, at::Tensor storage) {
+  void apply(const at::Tensor& in, at::Tensor out, at::Tensor storage,
+             const std::optional<c10::intrusive_ptr<FunctionLambda>>& func_between) {
     _fwd->apply(in, storage);
+    if (func_between.has_value() && *func_between) (*func_between)->apply({storage});
     _bwd->apply(storage, out);
   }
 
@@ -220,6 +242,14 @@ class Normal3DBlocksSVT : public torch::CustomClassHolder {
 
 }  // namespace ffi
 }  // namespace hasty
+
+// registered first: NufftNormal.apply takes a FunctionLambda (static initialisation runs in
+// definition order within this file)
+TORCH_LIBRARY(HastyInterface, hi) {
+  hi.class_<hasty::ffi::FunctionLambda>("FunctionLambda")
+      .def(torch::init<const std::string&, const std::string&, const std::vector<at::Tensor>&>())
+      .def("apply", &hasty::ffi::FunctionLambda::apply);
+}
 
 TORCH_LIBRARY(HastyNufft, hn) {
   hn.class_<hasty::ffi::NufftOptions>("NufftOptions")

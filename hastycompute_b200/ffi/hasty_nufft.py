@@ -35,7 +35,6 @@ class NufftNormal:
         self._nufftopt = _mod.NufftNormal(coord, list(nmodes), forward_opts._nufftopts, backward_opts._nufftopts)
 
     def apply(self, input: torch.Tensor, output: torch.Tensor, storage: torch.Tensor, callable=None):
-        if callable is not None:
-            raise RuntimeError("a function between the transforms is not supported; use the k-space manipulators "
-                               "of hastycompute_b200.batched_sense")
-        self._nufftopt.apply(input, output, storage)
+        """output = type1(f(type2(input))) with storage holding the k-space data in between;
+        f is `callable` (a FunctionLambda, applied in place) or the identity."""
+        self._nufftopt.apply(input, output, storage, callable._funclam if callable is not None else None)

@@ -51,3 +51,16 @@ def test_check_raises_with_message():
     code = lib.hb_plan_create(None, 16, 16, 16, 0)
     with pytest.raises(capi.HastyError, match="NULL"):
         capi.check(code)
+
+
+def test_function_lambda_runs_a_torchscript_function():
+    """HastyInterface.FunctionLambda (the reference's py_interface.cpp:6-15): a TorchScript
+    function compiled from source, called as entry(inout, captures), in place."""
+    import torch
+
+    from hastycompute_b200.ffi import hasty_interface as hi
+
+    script = "def apply(a: List[Tensor], b: List[Tensor]):\n    for i in range(len(b)):\n        a[i] += b[i]\n"
+    a = [torch.zeros(3), torch.ones(2)]
+    hi.FunctionLambda(script, "apply", [torch.arange(3.0), torch.full((2,), 2.0)]).apply(a)
+    assert torch.equal(a[0], torch.arange(3.0)) and torch.equal(a[1], torch.full((2,), 3.0))

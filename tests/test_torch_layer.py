@@ -163,6 +163,16 @@ def test_nufft_and_svt_torchscript_classes(cuda):
     st = torch.empty((1, K), dtype=torch.complex64, device=cuda)
     nn.apply(torch.from_numpy(x[None].astype(np.complex64)).to(cuda), y, st)
     assert O.rel_l2(_np(y[0]) / np.prod(shape), O.explicit_normal(x, coords_np)) < 1e-5
+    # a function between the transforms (py_nufft.cpp:96-107): here sample weights applied
+    # to the k-space data in place, captured by a TorchScript FunctionLambda
+    from hastycompute_b200.ffi import hasty_interface
+
+    w = rng.uniform(0.5, 1.5, K)
+    wt = torch.from_numpy(w.astype(np.complex64)).to(cuda)
+    scale = hasty_interface.FunctionLambda(
+        "def apply(a: List[Tensor], b: List[Tensor]):\n    a[0].mul_(b[0])\n", "apply", [wt])
+    nn.apply(torch.from_numpy(x[None].astype(np.complex64)).to(cuda), y, st, scale)
+    assert O.rel_l2(_np(y[0]) / np.prod(shape), O.explicit_normal(x, coords_np, weights=w)) < 1e-5
     with pytest.raises(RuntimeError, match="nmodes"):
         op.apply(torch.from_numpy(c.astype(np.complex64)).to(cuda), torch.empty((3, *shape), dtype=torch.complex64,
                                                                               device=cuda))
