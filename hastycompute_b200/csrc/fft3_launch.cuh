@@ -113,15 +113,23 @@ cudaError_t fft3_grid(int n0, int n1, int n2, const float2* tw, float2* grid, in
   const long long vol = (long long)n0 * n1 * n2;
   cudaError_t e = contig_any<DIR>(n2, grid, (long long)nt * n0 * n1, tw + n0 + n1, st, kind);
   if (e != cudaSuccess) return e;
-  e = strided_any<DIR>(n1, grid, n2, n2, n0, (long long)n1 * n2, nt, vol, tw + n0, st, kind);
-  if (e != cudaSuccess) return e;
+  if (n1 > 1) {  // a length-1 axis (the leading axes of a 1-D or 2-D plan) needs no transform
+    e = strided_any<DIR>(n1, grid, n2, n2, n0, (long long)n1 * n2, nt, vol, tw + n0, st, kind);
+    if (e != cudaSuccess) return e;
+  }
+  if (n0 == 1) return cudaSuccess;
   return strided_any<DIR>(n0, grid, (long long)n1 * n2, n2, n1, n2, nt, vol, tw, st, kind);
 }
 
-// Team twiddle tables of the three lengths, back to back (forward sign, FP64 rounded).
+// Team twiddle tables of the three lengths, back to back (forward sign, FP64 rounded); a
+// length-1 axis holds the single entry 1.
 inline std::vector<float2> team_tables(const int* n) {
   std::vector<float2> tw;
   for (int a = 0; a < 3; ++a) {
+    if (n[a] == 1) {
+      tw.push_back(make_float2(1.f, 0.f));
+      continue;
+    }
     int E = 0, S = 0;
     team_length(n[a], &E, &S);
     for (int k1 = 0; k1 < E; ++k1)

@@ -54,15 +54,21 @@ class Nufft : public torch::CustomClassHolder {
  public:
   Nufft(const at::Tensor& coords, const std::vector<int64_t>& nmodes, const c10::intrusive_ptr<NufftOptions>& opts)
       : _opts(opts), _nmodes(nmodes) {
-    if (nmodes.size() != 4) throw std::runtime_error("nmodes must be [ntransf, nz, ny, nx] (3-D transforms only)");
-    if (!coords.is_cuda() || coords.scalar_type() != at::kFloat || coords.dim() != 2 || coords.size(0) != 3)
-      throw std::runtime_error("Coordinates did not reside in cuda device as float32 [3, nfreq]");
+    // [ntransf, nz, ny, nx], [ntransf, ny, nx] or [ntransf, nx] (the reference's 3-D, 2-D and
+    // 1-D plans) with coords [ndim, nfreq]
+    const int64_t d = (int64_t)nmodes.size() - 1;
+    if (d < 1 || d > 3) throw std::runtime_error("nmodes must be [ntransf, nz, ny, nx], [ntransf, ny, nx] or [ntransf, nx]");
+    if (!coords.is_cuda() || coords.scalar_type() != at::kFloat || coords.dim() != 2 || coords.size(0) != d)
+      throw std::runtime_error("Coordinates did not reside in cuda device as float32 [ndim, nfreq]");
+    for (int64_t a = 1; a <= d; ++a)
+      if (d < 3 && nmodes[a] == 1) throw std::runtime_error("a transformed axis needs more than one mode");
     _coords = coords.contiguous();
     _nfreq = _coords.size(1);
     c10::cuda::CUDAGuard g(_coords.device());
     const int maxbatch = (int)std::max<int64_t>(1, std::min<int64_t>(nmodes[0], 16));
-    check(hb_nufft_create(&_plan, nmodes[1], nmodes[2], nmodes[3], _coords.data_ptr<float>(), _nfreq, opts->tol,
-                          maxbatch, _coords.device().index(), stream_of(_coords)));
+    const int64_t nz = d == 3 ? nmodes[1] : 1, ny = d >= 2 ? nmodes[d - 1] : 1, nx = nmodes[d];
+    check(hb_nufft_create(&_plan, nz, ny, nx, _coords.data_ptr<float>(), _nfreq, opts->tol, maxbatch,
+                          _coords.device().index(), stream_of(_coords)));
   }
   ~Nufft() override {
     if (_plan) hb_nufft_destroy(_plan);

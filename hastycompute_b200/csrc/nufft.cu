@@ -92,14 +92,18 @@ template <int W>
 cudaError_t spread_w(const hb_nufft* p, const float2* c, long long c_ld, int nb, cudaStream_t st) {
   dim3 grid((unsigned)((p->g.K + 255) / 256), nb);
   LaunchScope ls(HB_KERNEL_NUFFT, st);
-  nufft_spread_kernel<W><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, c, c_ld, p->grid);
+  if (p->g.dim == 3) nufft_spread_kernel<W, 3><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, c, c_ld, p->grid);
+  else if (p->g.dim == 2) nufft_spread_kernel<W, 2><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, c, c_ld, p->grid);
+  else nufft_spread_kernel<W, 1><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, c, c_ld, p->grid);
   return cudaGetLastError();
 }
 template <int W>
 cudaError_t interp_w(const hb_nufft* p, float2* c, long long c_ld, int nb, cudaStream_t st) {
   dim3 grid((unsigned)((p->g.K + 255) / 256), nb);
   LaunchScope ls(HB_KERNEL_NUFFT, st);
-  nufft_interp_kernel<W><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, p->grid, c, c_ld);
+  if (p->g.dim == 3) nufft_interp_kernel<W, 3><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, p->grid, c, c_ld);
+  else if (p->g.dim == 2) nufft_interp_kernel<W, 2><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, p->grid, c, c_ld);
+  else nufft_interp_kernel<W, 1><<<grid, 256, 0, st>>>(p->g, p->coords, p->perm, p->grid, c, c_ld);
   return cudaGetLastError();
 }
 
@@ -224,7 +228,13 @@ int hb_nufft_create(hb_nufft** out, int64_t nz, int64_t ny, int64_t nx, const fl
   g.w = width_for_tol(tol);
   g.beta = (float)(2.30 * g.w);
   g.K = nsamples;
+  // nz = 1: a 2-D plan over (ny, nx); nz = ny = 1: a 1-D plan over nx (coords [dim][K])
+  g.dim = nz != 1 ? 3 : (ny != 1 ? 2 : 1);
   for (int a = 0; a < 3; ++a) {
+    if (a < 3 - g.dim) {  // degenerate leading axis
+      g.N[a] = g.n[a] = g.nb[a] = 1;
+      continue;
+    }
     int E = 0, S = 0;
     const int64_t n = 2 * Nv[a];
     if (Nv[a] < 1 || n > 512 || !team_length((int)n, &E, &S) || n < 2 * g.w)
@@ -267,13 +277,19 @@ int hb_nufft_create(hb_nufft** out, int64_t nz, int64_t ny, int64_t nx, const fl
   // host tables: 1/phi_hat per axis and the team twiddles of each fine-grid length
   std::vector<float> corr;
   for (int a = 0; a < 3; ++a)
-    for (int i = 0; i < g.N[a]; ++i) corr.push_back((float)(1.0 / phi_hat(i - g.N[a] / 2, g.n[a], g.w, 2.30 * g.w)));
+    for (int i = 0; i < g.N[a]; ++i)
+      corr.push_back(a < 3 - g.dim ? 1.f : (float)(1.0 / phi_hat(i - g.N[a] / 2, g.n[a], g.w, 2.30 * g.w)));
   const std::vector<float2> tw = team_tables(g.n);
   if ((e = cudaMemcpyAsync(p->corr, corr.data(), corr.size() * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return bail(e, "upload");
   if ((e = cudaMemcpyAsync(p->tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return bail(e, "upload");
-  if ((e = cudaMemcpyAsync(p->coords, coords, 3 * nsamples * sizeof(float), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+  // the caller's [dim][K] rows become the trailing rows of [3][K]; degenerate rows are 0
+  const int lead = 3 - g.dim;
+  if (lead > 0 && (e = cudaMemsetAsync(p->coords, 0, lead * nsamples * sizeof(float), st)) != cudaSuccess)
+    return bail(e, "coords copy");
+  if ((e = cudaMemcpyAsync(p->coords + lead * nsamples, coords, g.dim * nsamples * sizeof(float),
+                           cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return bail(e, "coords copy");
   // counting sort of the samples by bin
   if ((e = cudaMemsetAsync(counts, 0, nbins * sizeof(int), st)) != cudaSuccess) return bail(e, "memset");

@@ -26,13 +26,16 @@ namespace hb {
 constexpr int kNufftBin = 8;  // fine-grid cells per bin edge
 constexpr float kNufftInvTwoPi = 0.159154943091895336f;
 
+// A plan of dimension d < 3 keeps the 3-axis layout with its leading 3 - d axes
+// degenerate (N = n = 1, one bin, coordinates 0, no spreading along them, correction 1).
 struct NufftGeom {
   int N[3];          // modes per axis
-  int n[3];          // fine grid per axis (2 N)
+  int n[3];          // fine grid per axis (2 N; 1 on a degenerate axis)
   int nb[3];         // bins per axis
   int w;             // kernel width (cells)
   float beta;        // kernel shape
   long long K;       // samples
+  int dim;           // 1, 2 or 3 transformed axes (the trailing ones)
 };
 
 __device__ __forceinline__ float nufft_grid_pos(float x, int n) {
@@ -109,28 +112,40 @@ __global__ void nufft_bin_scatter_kernel(long long K, const int* sample_bin, int
   perm[atomicAdd(&cursor[sample_bin[j]], 1)] = (int)j;
 }
 
+// Kernel weights of axis a, or the single weight 1 at cell 0 on a degenerate axis
+template <int W, int WA>
+__device__ __forceinline__ int nufft_axis(const NufftGeom& g, const float* coords, int a, int j, float* wt) {
+  if constexpr (WA == 1) {
+    wt[0] = 1.f;
+    return 0;
+  } else {
+    return nufft_axis_weights<W>(nufft_grid_pos(coords[a * g.K + j], g.n[a]), g.beta, wt);
+  }
+}
+
 // ---- type 1: spread (grid pre-zeroed); grid y = transform within the batch ----
-template <int W>
+template <int W, int DIM>
 __global__ void __launch_bounds__(256) nufft_spread_kernel(NufftGeom g, const float* coords, const int* perm,
                                                            const float2* c, long long c_ld, float2* grid) {
+  constexpr int W0 = DIM >= 3 ? W : 1, W1 = DIM >= 2 ? W : 1;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.K) return;
   const int j = perm[i];
   const float2 cj = c[(long long)blockIdx.y * c_ld + j];
-  float w0[W], w1[W], w2[W];
-  const int i0 = nufft_axis_weights<W>(nufft_grid_pos(coords[j], g.n[0]), g.beta, w0);
-  const int i1 = nufft_axis_weights<W>(nufft_grid_pos(coords[g.K + j], g.n[1]), g.beta, w1);
-  const int i2 = nufft_axis_weights<W>(nufft_grid_pos(coords[2 * g.K + j], g.n[2]), g.beta, w2);
+  float w0[W0], w1[W1], w2[W];
+  const int i0 = nufft_axis<W, W0>(g, coords, 0, j, w0);
+  const int i1 = nufft_axis<W, W1>(g, coords, 1, j, w1);
+  const int i2 = nufft_axis<W, W>(g, coords, 2, j, w2);
   float2* G = grid + (long long)blockIdx.y * g.n[0] * g.n[1] * g.n[2];
   int x2[W];
 #pragma unroll
   for (int m = 0; m < W; ++m) x2[m] = wrap(i2 + m, g.n[2]);
 #pragma unroll 1
-  for (int a = 0; a < W; ++a) {
+  for (int a = 0; a < W0; ++a) {
     const float2 ca = cscale(cj, w0[a]);
     float2* Ga = G + (long long)wrap(i0 + a, g.n[0]) * g.n[1] * g.n[2];
 #pragma unroll
-    for (int b = 0; b < W; ++b) {
+    for (int b = 0; b < W1; ++b) {
       const float2 cab = cscale(ca, w1[b]);
       float2* Gab = Ga + (long long)wrap(i1 + b, g.n[1]) * g.n[2];
 #pragma unroll
@@ -140,27 +155,28 @@ __global__ void __launch_bounds__(256) nufft_spread_kernel(NufftGeom g, const fl
 }
 
 // ---- type 2: interpolate ----
-template <int W>
+template <int W, int DIM>
 __global__ void __launch_bounds__(256) nufft_interp_kernel(NufftGeom g, const float* coords, const int* perm,
                                                            const float2* grid, float2* c, long long c_ld) {
+  constexpr int W0 = DIM >= 3 ? W : 1, W1 = DIM >= 2 ? W : 1;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.K) return;
   const int j = perm[i];
-  float w0[W], w1[W], w2[W];
-  const int i0 = nufft_axis_weights<W>(nufft_grid_pos(coords[j], g.n[0]), g.beta, w0);
-  const int i1 = nufft_axis_weights<W>(nufft_grid_pos(coords[g.K + j], g.n[1]), g.beta, w1);
-  const int i2 = nufft_axis_weights<W>(nufft_grid_pos(coords[2 * g.K + j], g.n[2]), g.beta, w2);
+  float w0[W0], w1[W1], w2[W];
+  const int i0 = nufft_axis<W, W0>(g, coords, 0, j, w0);
+  const int i1 = nufft_axis<W, W1>(g, coords, 1, j, w1);
+  const int i2 = nufft_axis<W, W>(g, coords, 2, j, w2);
   const float2* G = grid + (long long)blockIdx.y * g.n[0] * g.n[1] * g.n[2];
   int x2[W];
 #pragma unroll
   for (int m = 0; m < W; ++m) x2[m] = wrap(i2 + m, g.n[2]);
   float2 acc = make_float2(0.f, 0.f);
 #pragma unroll 1
-  for (int a = 0; a < W; ++a) {
+  for (int a = 0; a < W0; ++a) {
     const float2* Ga = G + (long long)wrap(i0 + a, g.n[0]) * g.n[1] * g.n[2];
     float2 sa = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int b = 0; b < W; ++b) {
+    for (int b = 0; b < W1; ++b) {
       const float2* Gab = Ga + (long long)wrap(i1 + b, g.n[1]) * g.n[2];
       float2 sb = make_float2(0.f, 0.f);
 #pragma unroll

@@ -53,22 +53,27 @@ class NufftOptions:
 
 
 class NufftPlan:
-    """A plan for modes (nz, ny, nx) at fixed sample coordinates (``hb_nufft``):
-    coords float32 [3, nsamples] on a CUDA device, row a pairing with image axis a."""
+    """A plan for modes ``nmodes`` = (nz, ny, nx), (ny, nx) or (nx,) at fixed sample
+    coordinates (``hb_nufft``): coords float32 [len(nmodes), nsamples] on a CUDA device, row
+    a pairing with image axis a (the reference's 1-D, 2-D and 3-D plans)."""
 
     def __init__(self, coords, nmodes, tol=1e-5, maxbatch=8):
         self.lib = capi.load()
-        if coords.dim() != 2 or coords.shape[0] != 3:
-            raise RuntimeError("coords must be [3, nsamples] (only 3-D transforms are supported)")
+        self.shape = tuple(int(n) for n in nmodes)
+        d = len(self.shape)
+        if d not in (1, 2, 3) or coords.dim() != 2 or coords.shape[0] != d:
+            raise RuntimeError("coords must be [ndim, nsamples] with ndim = len(nmodes) in 1..3")
         if coords.dtype != torch.float32 or coords.device.type != "cuda":
             raise RuntimeError("coords must be float32 on a CUDA device")
+        if d < 3 and 1 in self.shape:
+            raise RuntimeError("a transformed axis needs more than one mode")
         self.coords = coords.contiguous()
         self.device = self.coords.device
-        self.shape = tuple(int(n) for n in nmodes)
         self.nfreq = int(coords.shape[1])
         self._h = None
         h = ctypes.c_void_p()
-        capi.check(self.lib.hb_nufft_create(ctypes.byref(h), *self.shape, _ptr(self.coords), self.nfreq,
+        dims3 = (1,) * (3 - d) + self.shape  # leading axes of length 1 select the 2-D / 1-D plan
+        capi.check(self.lib.hb_nufft_create(ctypes.byref(h), *dims3, _ptr(self.coords), self.nfreq,
                                             float(tol), int(maxbatch), self.device.index, _stream_ptr(self.device)))
         self._h = h
 
@@ -169,12 +174,13 @@ class NufftPlan:
 
 
 class CUDANufft:
-    """``hasty::fft::CUDANufft`` (``nufft.ixx:108-160``): ``nmodes = [ntransf, nz, ny, nx]``."""
+    """``hasty::fft::CUDANufft`` (``nufft.ixx:108-160``): ``nmodes = [ntransf, nz, ny, nx]``,
+    ``[ntransf, ny, nx]`` or ``[ntransf, nx]`` with coords [3|2|1, nfreq]."""
 
     def __init__(self, coords, nmodes, opts=None):
         opts = NufftOptions() if opts is None else opts
-        if len(nmodes) != 4:
-            raise RuntimeError("nmodes must be [ntransf, nz, ny, nx]")
+        if len(nmodes) not in (2, 3, 4):
+            raise RuntimeError("nmodes must be [ntransf, nz, ny, nx], [ntransf, ny, nx] or [ntransf, nx]")
         self._ntransf = int(nmodes[0])
         self._nmodes = [int(n) for n in nmodes]
         self._opts = opts
@@ -198,7 +204,7 @@ class CUDANufft:
         return self._plan.nfreq
 
     def ndim(self):
-        return 3
+        return len(self._nmodes) - 1
 
     def close(self):
         self._plan.close()

@@ -189,6 +189,8 @@ class ReconServer:
                 t.join()
             for w in list(self._workers.values()):
                 w.thread.join()
+                w.batch = None  # the running batch's workspace goes back to the allocator
+            self._workers.clear()
         if self._errors:
             raise self._errors[0]
 

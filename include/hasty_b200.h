@@ -297,6 +297,9 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
  * method of finufft); kernel width w = ceil(log10(1/tol)) + 1 fine-grid cells.
  * 2*N_a must be one of 8, 16, 32, 64, 128, 256, 512, 96, 160, 192, 320 and >= 2w.
  * Type 1 accumulates with atomics, so its last bits vary from run to run.
+ * Lower dimensions (the reference's 1-D and 2-D plans, nufft.ixx:72-160): nz = 1 makes a
+ * 2-D plan over (ny, nx) and nz = ny = 1 a 1-D plan over nx; coords is then [2][nsamples]
+ * or [1][nsamples] (rows pairing with the transformed axes in order).
  *
  * hb_nufft_create copies coords, sorts the samples by fine-grid bin and allocates the
  * fine grids of `maxbatch` (1..32) transforms plus as many mode and k-space arrays; it synchronises

@@ -157,28 +157,37 @@ def explicit_normal(x, coords, weights=None):
     return y / float(np.prod(N))
 
 
+_AXES = "zyx"
+
+
 def nudft_type1(coords, c, nmodes, isign=+1):
     """Direct FP64 type-1 NUDFT, the transform ``hasty::fft::CUDANufft`` type 1 computes
     through cufinufft (``lib/fft/nufft.cpp:640-700``; options ``nufft.ixx:46-48``):
     f[t, k] = sum_j c[t, j] exp(isign * i * k . x_j), centred modes k = i - n//2,
-    c [ntransf, K] -> f [ntransf, *nmodes]."""
+    c [ntransf, K] -> f [ntransf, *nmodes]; d = len(nmodes) = coords.shape[0] in 1..3 (the
+    reference's 1-D, 2-D and 3-D plans, ``nufft.ixx:72-160``)."""
     coords = np.asarray(coords, np.float64)
     c = np.atleast_2d(np.asarray(c, np.complex128))
+    d = len(nmodes)
     k = [np.arange(n) - n // 2 for n in nmodes]
-    e = [np.exp(isign * 1j * np.outer(coords[a], k[a])) for a in range(3)]
-    return np.einsum("tj,jz,jy,jx->tzyx", c, e[0], e[1], e[2], optimize=True)
+    e = [np.exp(isign * 1j * np.outer(coords[a], k[a])) for a in range(d)]
+    ax = _AXES[3 - d:]
+    return np.einsum("tj," + ",".join("j" + a for a in ax) + "->t" + ax, c, *e, optimize=True)
 
 
 def nudft_type2(coords, f, isign=-1):
     """Direct FP64 type-2 NUDFT (``lib/fft/nufft.cpp:702-767``):
-    c[t, j] = sum_k f[t, k] exp(isign * i * k . x_j), f [ntransf, *nmodes] -> c [ntransf, K]."""
+    c[t, j] = sum_k f[t, k] exp(isign * i * k . x_j), f [ntransf, *nmodes] -> c [ntransf, K]
+    (d = coords.shape[0] transformed axes, 1..3)."""
     coords = np.asarray(coords, np.float64)
+    d = coords.shape[0]
     f = np.asarray(f, np.complex128)
-    if f.ndim == 3:
+    if f.ndim == d:
         f = f[None]
     k = [np.arange(n) - n // 2 for n in f.shape[1:]]
-    e = [np.exp(isign * 1j * np.outer(coords[a], k[a])) for a in range(3)]
-    return np.einsum("tzyx,jz,jy,jx->tj", f, e[0], e[1], e[2], optimize=True)
+    e = [np.exp(isign * 1j * np.outer(coords[a], k[a])) for a in range(d)]
+    ax = _AXES[3 - d:]
+    return np.einsum("t" + ax + "," + ",".join("j" + a for a in ax) + "->tj", f, *e, optimize=True)
 
 
 def sense_adjoint(coords, kdata, smaps, coils=None):

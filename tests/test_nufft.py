@@ -51,6 +51,27 @@ def test_type1_type2_against_direct_nudft(cuda, shape, tol, bound):
     assert O.rel_l2(_np(cc), ref2) < bound
 
 
+@pytest.mark.parametrize("shape", [(32, 16), (8, 64), (64,), (16,)])
+def test_lower_dimensional_plans_against_direct_nudft(cuda, shape):
+    """The reference's 2-D and 1-D plans (nufft.ixx:72-160): coords [d, K], modes [ntransf, *shape]."""
+    d, K = len(shape), 1500
+    rng = np.random.default_rng(7)
+    coords = rng.uniform(-np.pi, np.pi, (d, K)).astype(np.float32)
+    ct = torch.from_numpy(coords).to(cuda)
+    plan = NufftPlan(ct, shape, tol=1e-6, maxbatch=2)
+    c = _rand((3, K), 8)
+    assert O.rel_l2(_np(plan.type1(_c64(c, cuda))), O.nudft_type1(coords, c, shape, +1)) < 1e-5
+    fm = _rand((3,) + shape, 9)
+    assert O.rel_l2(_np(plan.type2(_c64(fm, cuda))), O.nudft_type2(coords, fm, -1)) < 1e-5
+    # the reference-named mirror with nmodes [ntransf, *shape]
+    op = CUDANufft(ct, [2, *shape], NufftOptions.type2())
+    out = torch.empty((2, K), dtype=torch.complex64, device=cuda)
+    op.apply(_c64(fm[:2], cuda), out)
+    assert op.ndim() == d and O.rel_l2(_np(out), O.nudft_type2(coords, fm[:2], -1)) < 1e-5
+    with pytest.raises(RuntimeError):
+        NufftPlan(ct[:1] if d == 2 else torch.cat([ct, ct]), shape)  # rows must match the dimension
+
+
 def test_signs_batching_and_periodicity(cuda):
     shape, K = (16, 16, 16), 1800
     coords = _coords(K, 4)

@@ -205,3 +205,21 @@ def test_torch_fp64_restatement_matches_numpy(golden):
     xn, nn = O.conjugate_gradient(An, a, iters=6)
     xt, nt = O.conjugate_gradient(At, torch.from_numpy(a), iters=6)
     assert nn == nt == 6 and O.rel_l2(xt, xn) < 1e-12
+
+
+def test_lower_dimensional_nudft_matches_a_direct_sum():
+    """The oracle's 2-D and 1-D NUDFTs (the reference's lower-dimensional plans) against an
+    explicit double loop / single loop."""
+    rng = np.random.default_rng(11)
+    for shape in [(4, 6), (5,)]:
+        d = len(shape)
+        x = rng.uniform(-np.pi, np.pi, (d, 7))
+        c = rng.standard_normal((2, 7)) + 1j * rng.standard_normal((2, 7))
+        f = O.nudft_type1(x, c, shape, +1)
+        k = np.stack(np.meshgrid(*[np.arange(n) - n // 2 for n in shape], indexing="ij"), axis=-1)
+        want = np.einsum("tj,...j->t...", c, np.exp(1j * np.tensordot(k, x, axes=([-1], [0]))))
+        assert np.allclose(f, want, atol=1e-12)
+        g = rng.standard_normal((2,) + shape) + 1j * rng.standard_normal((2,) + shape)
+        c2 = O.nudft_type2(x, g, -1)
+        want2 = g.reshape(2, -1) @ np.exp(-1j * np.tensordot(k, x, axes=([-1], [0]))).reshape(-1, 7)
+        assert np.allclose(c2, want2, atol=1e-12)
