@@ -1357,8 +1357,6 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
   if (!hb_size_supported(nz, ny, nx))
     return fail(HB_ERR_UNSUPPORTED, "hb_toeplitz_apply_noalloc: image size not supported");
   if (!in || !out || !packed_diag) return fail(HB_ERR_INVALID, "hb_toeplitz_apply_noalloc: NULL pointer");
-  if (!diag_aligned(packed_diag))
-    return fail(HB_ERR_INVALID, "hb_toeplitz_apply_noalloc: packed diagonal not 16-byte aligned");
   const unsigned long long need = 16ull * (unsigned long long)(nz * ny * nx);
   if (need > HB_NOALLOC_SCRATCH_BYTES)
     return fail(HB_ERR_WORKSPACE, "hb_toeplitz_apply_noalloc: " + std::to_string(nz) + "x" + std::to_string(ny) + "x" +
@@ -1366,6 +1364,8 @@ int hb_toeplitz_apply_noalloc(int64_t nz, int64_t ny, int64_t nx, const void* in
                                       " bytes of scratch, more than the built-in " +
                                       std::to_string((unsigned long long)HB_NOALLOC_SCRATCH_BYTES) +
                                       " (use hb_toeplitz_apply with a caller workspace)");
+  if (!diag_aligned(packed_diag))
+    return fail(HB_ERR_INVALID, "hb_toeplitz_apply_noalloc: packed diagonal not 16-byte aligned");
   // the built-in twiddle-table array holds the tables of axes up to 160; a size whose
   // tables would not fit is refused before anything is written
   if (table_offsets((int)nz, (int)ny, (int)nx).total > kNoAllocMaxTables)
