@@ -63,11 +63,11 @@ def test_lower_dimensional_plans_against_direct_nudft(cuda, shape):
     assert O.rel_l2(_np(plan.type1(_c64(c, cuda))), O.nudft_type1(coords, c, shape, +1)) < 1e-5
     fm = _rand((3,) + shape, 9)
     assert O.rel_l2(_np(plan.type2(_c64(fm, cuda))), O.nudft_type2(coords, fm, -1)) < 1e-5
-    # the reference-named mirror with nmodes [ntransf, *shape]
+    # the reference-named mirror with nmodes [ntransf, *shape] (default tol 1e-5: bound 10x)
     op = CUDANufft(ct, [2, *shape], NufftOptions.type2())
     out = torch.empty((2, K), dtype=torch.complex64, device=cuda)
     op.apply(_c64(fm[:2], cuda), out)
-    assert op.ndim() == d and O.rel_l2(_np(out), O.nudft_type2(coords, fm[:2], -1)) < 1e-5
+    assert op.ndim() == d and O.rel_l2(_np(out), O.nudft_type2(coords, fm[:2], -1)) < 1e-4
     with pytest.raises(RuntimeError):
         NufftPlan(ct[:1] if d == 2 else torch.cat([ct, ct]), shape)  # rows must match the dimension
 
