@@ -1,6 +1,5 @@
-// Bulk asynchronous copies between global and shared memory on the TMA engine (the untiled
-// cp.async.bulk and the tiled cp.async.bulk.tensor through a tensor map) and the mbarriers
-// that track them.  No cluster multicast anywhere:
+// Bulk asynchronous copies between global and shared memory (the TMA engine's untiled
+// form, cp.async.bulk) and the mbarriers that track them.  No cluster multicast anywhere:
 // every copy moves this CTA's own tile of this GPU's own memory.
 //
 // Every wait is bounded: mbar_wait gives up after about one second of SM clocks (or once
@@ -63,23 +62,6 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 // this thread's bulk stores are complete
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-// Tiled tensor copies through a 4-D tensor map (coordinates innermost first; the innermost
-// coordinate times the element size must be a multiple of 16 bytes).  `map` is the generic
-// address of a CUtensorMap in kernel parameter, constant or global memory.
-__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* map, int c0, int c1, int c2, int c3,
-                                            uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-      "[%6];" ::"r"(dst),
-      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
-      : "memory");
-}
-__device__ __forceinline__ void tma_store_4d(const void* map, uint32_t src, int c0, int c1, int c2, int c3) {
-  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(map),
-               "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(src)
-               : "memory");
-}
-
 // generic-proxy writes to shared memory become visible to the bulk-copy (async) proxy
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 

@@ -10,8 +10,6 @@
 #include <string>
 #include <vector>
 
-#include <cudaTypedefs.h>
-
 #include "../../include/hasty_b200.h"
 #include "cg_kernels.cuh"
 #include "diag_kernels.cuh"
@@ -312,9 +310,6 @@ int run_normal(const hb_plan* p, PassArgs a, cudaStream_t st) {
   const int ia = axis_index(p->N2), iy = ilog2(yt) - 3;
   const int nslots = a.nslots;
   if (nslots > 65535) return fail(HB_ERR_INVALID, "too many system x coil slots in one launch (max 65535)");
-  if (a.map_status)
-    return fail(HB_ERR_CUDA, a.map_status == 1 ? "spill tensor map: cuTensorMapEncodeTiled unavailable from the driver"
-                                               : "spill tensor map: cuTensorMapEncodeTiled rejected the spill layout");
   cudaError_t e = p->precision == HB_PRECISION_BF16X3 ? launch_a_tc(p, a, st) : kLaunchA[ia][iy](a, a.nsys, st);
   if (e != cudaSuccess) return fail(HB_ERR_CUDA, std::string("pass A: ") + cudaGetErrorString(e));
   e = plane_launcher(p)(a, nslots, st);
@@ -458,37 +453,6 @@ int upload_tables(const hb_plan* p, const GroupWs& w, const hb_system* sys, int6
   return HB_OK;
 }
 
-// cuTensorMapEncodeTiled from the driver (through the runtime's entry-point lookup, so the
-// library needs no link against libcuda)
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      f = nullptr;
-    return (PFN_cuTensorMapEncodeTiled_v12000)f;
-  }();
-  return fn;
-}
-
-// The tensor map through which passes A and C copy their spill tiles: the spill as the 4-D
-// tensor {y: N1, kx: M2, z: N0, slot: nslots} of 8-byte elements, boxes of YT y values by
-// M2 / spill_boxes(M2) kx rows, 128-byte swizzle when a box row is 128 bytes (YT = 16).
-int encode_spill_map(CUtensorMap* m, float2* spill, int N0, int N1, int N2, int64_t nslots) {
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc) return 1;
-  const int M2 = 2 * N2, YT = spill_yt(N1);
-  const cuuint64_t dims[4] = {(cuuint64_t)N1, (cuuint64_t)M2, (cuuint64_t)N0, (cuuint64_t)(nslots > 0 ? nslots : 1)};
-  const cuuint64_t strides[3] = {(cuuint64_t)N1 * 8, (cuuint64_t)M2 * N1 * 8, (cuuint64_t)N0 * M2 * N1 * 8};
-  const cuuint32_t box[4] = {(cuuint32_t)YT, (cuuint32_t)(M2 / spill_boxes(M2)), 1, 1};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)spill, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, YT == 16 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS ? 0 : 2;
-}
-
 PassArgs group_pass_args(const hb_plan* p, const GroupWs& w, int64_t g, int64_t slots, bool iter_inputs) {
   PassArgs a{};
   a.N0 = p->N0; a.N1 = p->N1; a.N2 = p->N2;
@@ -513,7 +477,6 @@ PassArgs group_pass_args(const hb_plan* p, const GroupWs& w, int64_t g, int64_t 
   a.accumulate = 0;
   a.dot_partials = nullptr;
   a.wait_error = p->tc_wait_error;
-  a.map_status = encode_spill_map(&a.spill_map, w.spill, p->N0, p->N1, p->N2, slots);
   return a;
 }
 

@@ -1,7 +1,8 @@
 // Pass A on the 5th-generation tensor cores (tcgen05): the zero-padded 2nx-point DFT along
 // x as a dense contraction, for nx = ny = 128.
 //
-//   spill[slot][z][kx][y] = sum_{x < nx} F[kx][x] * (S_c * x)[z][y][x],  F[kx][x] = e^{-2 pi i kx x / 2nx}
+//   spill(slot, z, kx, y) = sum_{x < nx} F[kx][x] * (S_c * x)[z][y][x],  F[kx][x] = e^{-2 pi i kx x / 2nx}
+// (stored at spill_index, the tiled layout passes B and C read)
 //
 // One CTA per (slot, z): D^T[y][kx] = A[y][x] . F[kx][x]^T with A = S_c * x (M = 128
 // lines y, N = 256 frequencies kx, K = 128 samples x), so every sample is loaded and split
@@ -316,7 +317,8 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 1) expand_fwd_x_tc_kernel(Pas
       // epilogue: warp w reads TMEM lanes [32 (w % 4), +32) = lines y, columns (kx) of half w / 4
       const int q = warp % 4, ch = warp / 4;
       const int y = q * 32 + lane;
-      float2* dst = a.spill + spill_index(slot, z, 0, y, N0, N1, M2);
+      constexpr int YT = spill_yt(kRows);
+      float2* dst = a.spill + spill_tile_offset(slot, z, y / YT, N0, N1, M2);  // y's spill tile
 #pragma unroll 1
       for (int cb = 0; cb < kCols / 32; ++cb) {
         const int c0 = ch * (kCols / 2) + cb * 16;
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(tc::kThreadsAll, 1) expand_fwd_x_tc_kernel(Pas
         tmem_ld_wait();
 #pragma unroll
         for (int j = 0; j < 16; ++j)
-          dst[(long long)(c0 + j) * N1] = make_float2(__uint_as_float(re[j]), __uint_as_float(im[j]));
+          dst[spill_in_tile(c0 + j, y % YT, YT)] = make_float2(__uint_as_float(re[j]), __uint_as_float(im[j]));
       }
     }
   }

@@ -20,7 +20,6 @@
 #pragma once
 
 #include <cooperative_groups.h>
-#include <cuda.h>
 
 #include "bulk.cuh"
 #include "common.cuh"
@@ -30,38 +29,43 @@ namespace hb {
 
 // ------------------------------------------------------------------- spill layout ----
 // The spill holds, per (system, coil) slot, the image after the forward x transform:
-// [slot][z][kx][y].  Row z of the (slot, kx) plane that pass B transforms is N1 contiguous
-// values, M2 * N1 apart from row z + 1.  The (slot, z, y-tile) tile that a pass-A or pass-C
-// CTA moves ([kx][y0, y0 + YT), M2 rows of YT values, N1 apart) travels as tensor copies
-// (cp.async.bulk.tensor, one box of up to 256 kx rows) through a 4-D tensor map
-// {y: N1, kx: M2, z: N0, slot}; with YT = 16 the map swizzles the 16-byte chunks of each
-// 128-byte kx row by (kx mod 8), so a tile column (one y, consecutive kx: what one FFT team
-// writes in pass A and reads in pass C) falls on distinct shared-memory banks.
+// [slot][z][yt][kx][yy'] with yt = y / YT, yy' = (y % YT) ^ (kx % YT), YT = spill_yt(N1).
+// * The (slot, z, yt) tile that passes A and C move is one contiguous M2 x YT block, so it
+//   travels as one bulk copy and lies in shared memory exactly as in global memory.
+// * The XOR puts the YT values of one kx row in an order that depends on kx, so a tile
+//   column (one y, consecutive kx: what one FFT team writes or reads) falls on distinct
+//   shared-memory banks without padding.
+// * Row z of the (slot, kx) plane that pass B transforms is N1 / YT chunks of YT values
+//   (128 bytes for YT = 16), M2 * YT apart, rows M2 * N1 apart.
 __host__ __device__ constexpr int spill_yt(int N1) { return N1 < 16 ? N1 : 16; }
+__host__ __device__ inline long long spill_tile_offset(int slot, int z, int yt, int N0, int N1, int M2) {
+  const int YT = spill_yt(N1);
+  return (((long long)slot * N0 + z) * (N1 / YT) + yt) * (long long)(M2 * YT);
+}
+__host__ __device__ constexpr int spill_in_tile(int kx, int yy, int YT) { return kx * YT + (yy ^ (kx & (YT - 1))); }
 __host__ __device__ inline long long spill_index(int slot, int z, int kx, int y, int N0, int N1, int M2) {
-  return (((long long)slot * N0 + z) * M2 + kx) * N1 + y;
+  const int YT = spill_yt(N1);
+  return spill_tile_offset(slot, z, y / YT, N0, N1, M2) + spill_in_tile(kx, y % YT, YT);
 }
-// Position of element (kx, yy) of a tile in shared memory (float2 units): the tensor map's
-// SWIZZLE_128B pattern for YT = 16 (each box starts on a 1024-byte boundary, so the 8-row
-// swizzle atom follows kx), dense rows otherwise.
-template <int YT>
-__host__ __device__ constexpr int tile_pos(int kx, int yy) {
-  if constexpr (YT == 16) return kx * 16 + ((((yy >> 1) ^ (kx & 7)) << 1) | (yy & 1));
-  else return kx * YT + yy;
-}
-// kx rows per tensor-copy box (box dimensions are at most 256): M2 / spill_boxes(M2)
-__host__ __device__ constexpr int spill_boxes(int M2) { return (M2 + 255) / 256; }
 
-// Rows of one (slot, kx) plane of the spill, for pass B.
+// Rows of one (slot, kx) plane of the spill, for pass B (N1 a compile-time constant).
 template <int N1>
 struct SpillPlane {
-  float2* base;    // element (z, y) at base + z * rs + y
+  static constexpr int YT = spill_yt(N1);
+  float2* base;    // element (z, y) at base + z * rs + (y / YT) * cs + ((y % YT) ^ sw)
   long long rs;    // z pitch: M2 * N1
+  long long cs;    // y-chunk pitch: M2 * YT
+  int sw;          // kx % YT
   __device__ __forceinline__ SpillPlane(float2* spill, int slot, int kx, int N0, int M2) {
-    base = spill + spill_index(slot, 0, kx, 0, N0, N1, M2);
+    base = spill + spill_tile_offset(slot, 0, 0, N0, N1, M2) + (long long)kx * YT;
     rs = (long long)M2 * N1;
+    cs = (long long)M2 * YT;
+    sw = kx & (YT - 1);
   }
-  __device__ __forceinline__ float2& at(int z, int y) const { return base[z * rs + y]; }
+  __device__ __forceinline__ long long off(int z, int y) const {
+    return z * rs + (long long)(y / YT) * cs + ((y % YT) ^ sw);
+  }
+  __device__ __forceinline__ float2& at(int z, int y) const { return base[off(z, y)]; }
 };
 
 // ---------------------------------------------------------------- launch geometry ----
@@ -76,30 +80,20 @@ struct XPassCfg {
   static constexpr int THREADS = YT * S / LPT;
   static constexpr int NTEAMS = THREADS / S;
   static constexpr int TBUF = team_buf_stride<M2>();
-  static constexpr int TILE_ELEMS = M2 * YT;           // one spill tile in shared memory
+  static constexpr int TILE_ELEMS = M2 * YT;           // one spill tile, dense (swizzled)
   static constexpr unsigned TILE_BYTES = TILE_ELEMS * 8u;
-  static constexpr int NBOX = spill_boxes(M2), BOX_KX = M2 / NBOX;  // tensor-copy boxes of a tile
-  static constexpr int ALIGN_F2 = 128;  // dynamic shared memory is rounded up to 1024 bytes
   // pass A: the tile; the same space serves as the teams' FFT exchange buffers
-  static constexpr int TILE_RAW = (TILE_ELEMS > NTEAMS * TBUF) ? TILE_ELEMS : NTEAMS * TBUF;
-  static constexpr int TILE = (TILE_RAW + 127) / 128 * 128;  // keeps what follows 1024-byte aligned
+  static constexpr int TILE = (TILE_ELEMS > NTEAMS * TBUF) ? TILE_ELEMS : NTEAMS * TBUF;
   static constexpr int SMT = YT * N2;     // one coil's map rows [y][x]
   // float2 slots of dynamic shared memory: pass A = one tile (also the exchange buffers)
   // + two coil-map stages; pass C = two tiles + the exchange buffers; each + the M2-entry
   // twiddle table
-  static constexpr int SMEM_F2 = TILE + 2 * SMT + M2 + ALIGN_F2;
-  static constexpr int SMEM_F2_C = 2 * TILE_ELEMS + NTEAMS * TBUF + M2 + ALIGN_F2;
+  static constexpr int SMEM_F2 = TILE + 2 * SMT + M2;
+  static constexpr int SMEM_F2_C = 2 * TILE_ELEMS + NTEAMS * TBUF + M2;
   static_assert(THREADS % 32 == 0, "x-pass CTA must be whole warps");
   static_assert((YT & (YT - 1)) == 0, "the tile swizzle needs a power-of-two tile height");
   static_assert(TILE_BYTES % 16 == 0 && (SMT * 8) % 16 == 0, "bulk copies move whole 16-byte units");
-  static_assert(M2 % NBOX == 0 && (BOX_KX * YT * 8) % 1024 == 0, "each box starts on a 1024-byte boundary");
 };
-
-// The dynamic shared memory of the x passes, rounded up to a 1024-byte boundary (swizzled
-// tensor-copy destinations need it; the launch adds the slack).
-__device__ __forceinline__ float2* align_smem_1024(float2* p) {
-  return (float2*)(((uintptr_t)p + 1023) & ~(uintptr_t)1023);
-}
 
 // Row handled by team j of a row stage: the teams sharing a half-warp take rows S apart,
 // so their (odd-pitch) plane rows start on disjoint shared-memory banks.
@@ -186,10 +180,8 @@ struct PassArgs {
   const float* const* sys_diag;    // [nsys] packed diagonal [M2][2][N1][M0]
   const float* sys_lambda;         // [nsys] adds lambda * x (nullable = 0)
   const float2* mul;               // [N0][N1][N2] unconjugated multiplier (single system, nullable)
-  float2* spill;                   // [nslots][N0][M2][N1], see spill_index
+  float2* spill;                   // [nslots][N0][N1/YT][M2][YT], see spill_index
   int* wait_error;                 // set to 1 when a pass gave up waiting for a bulk copy
-  CUtensorMap spill_map;           // the spill as {y: N1, kx: M2, z: N0, slot} (tile copies of passes A, C)
-  int map_status;                  // host: 0 when spill_map was encoded
   const float2* tables;            // twiddle tables, see table_offsets
   long long out_ldz, out_ldy;      // element strides of every output image
   int accumulate;                  // 1: out += result, 0: out = result
@@ -202,12 +194,11 @@ struct PassArgs {
 // Per (system, z, y-tile): the x lines stay in registers while the coils stream by; coil
 // c + 1's map rows are copied asynchronously while coil c is transformed and stored.
 template <int N2, int YT>
-__global__ void __launch_bounds__(XPassCfg<N2, YT>::THREADS, 3)
-expand_fwd_x_kernel(const __grid_constant__ PassArgs a) {
+__global__ void __launch_bounds__(XPassCfg<N2, YT>::THREADS)
+expand_fwd_x_kernel(PassArgs a) {
   using C = XPassCfg<N2, YT>;
   constexpr int M2 = C::M2, E = C::E, S = C::S, LPT = C::LPT;
-  extern __shared__ __align__(128) float2 smem_raw[];
-  float2* smem = align_smem_1024(smem_raw);
+  extern __shared__ __align__(128) float2 smem[];
   float2* tile = smem;                // spill tile [M2][YT] (swizzled) / exchange buffers
   float2* smt = tile + C::TILE;       // 2 x [YT][N2] coil-map stages
   float2* tw = smt + 2 * C::SMT;      // [M2]
@@ -315,14 +306,13 @@ expand_fwd_x_kernel(const __grid_constant__ PassArgs a) {
     for (int l = 0; l < LPT; ++l) {
       const int line = team + l * C::NTEAMS;
 #pragma unroll
-      for (int r = 0; r < E; ++r) tile[tile_pos<YT>(dout_index<M2>(t, r), line)] = v[l][r];
+      for (int r = 0; r < E; ++r) tile[spill_in_tile(dout_index<M2>(t, r), line, YT)] = v[l][r];
     }
-    fence_proxy_async_smem();  // the tile's writes become visible to the tensor copy
+    fence_proxy_async_smem();  // the tile's writes become visible to the bulk copy
     __syncthreads();
     if (threadIdx.x == 0) {
-#pragma unroll
-      for (int b = 0; b < C::NBOX; ++b)
-        tma_store_4d(&a.spill_map, smem_u32(tile + b * C::BOX_KX * YT), y0, b * C::BOX_KX, z, slot0 + ci);
+      bulk_copy_s2g(a.spill + spill_tile_offset(slot0 + ci, z, blockIdx.x, N0, N1, M2), smem_u32(tile),
+                    C::TILE_BYTES);
       bulk_commit();
     }
   }
@@ -357,13 +347,14 @@ __device__ __forceinline__ void load_tcol(float* dst, const float* col, int t) {
   }
 }
 
-// L2 prefetch (a hint) of rows [r0, r0 + nrows) of a spill plane, N1 values each, in
-// 128-byte lines spread over the CTA's threads
+// L2 prefetch (a hint) of rows [r0, r0 + nrows) of a spill plane: each row is N1 / YT
+// chunks of YT values (YT * 8 bytes, at least 64), one prefetch per chunk, spread over the
+// CTA's threads
 template <int THREADS, int N1>
 __device__ __forceinline__ void prefetch_plane_rows_l2(const SpillPlane<N1>& pl, int r0, int nrows) {
-  constexpr int LINES = N1 * (int)sizeof(float2) / 128 > 0 ? N1 * (int)sizeof(float2) / 128 : 1;
-  for (int i = threadIdx.x; i < nrows * LINES; i += THREADS) {
-    const char* p = (const char*)(pl.base + (r0 + i / LINES) * pl.rs) + (i % LINES) * 128;
+  constexpr int YT = SpillPlane<N1>::YT, CH = N1 / YT;
+  for (int i = threadIdx.x; i < nrows * CH; i += THREADS) {
+    const float2* p = pl.base + (r0 + i / CH) * pl.rs + (long long)(i % CH) * pl.cs;
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
   }
 }
@@ -792,11 +783,10 @@ plane_mod_kernel(PassArgs a) {
 // ------------------------------------------------------------------------ pass C ----
 template <int N2, int YT>
 __global__ void __launch_bounds__(XPassCfg<N2, YT>::THREADS)
-inv_x_combine_kernel(const __grid_constant__ PassArgs a) {
+inv_x_combine_kernel(PassArgs a) {
   using C = XPassCfg<N2, YT>;
   constexpr int M2 = C::M2, E = C::E, S = C::S, LPT = C::LPT;
-  extern __shared__ __align__(128) float2 smem_raw[];
-  float2* smem = align_smem_1024(smem_raw);
+  extern __shared__ __align__(128) float2 smem[];
   float2* tiles = smem;                          // 2 x spill tile [M2][YT] (swizzled)
   float2* xbuf = tiles + 2 * C::TILE_ELEMS;      // teams' exchange buffers
   float2* tw = xbuf + C::NTEAMS * C::TBUF;
@@ -824,14 +814,12 @@ inv_x_combine_kernel(const __grid_constant__ PassArgs a) {
   const long long plane = (long long)N1 * N2;
 
   const int slot0 = a.sys_slot0[sys], ncoil = a.sys_nslot[sys];
-  // the tensor copies of coil ci's spill tile into tiles[ci & 1] (thread 0)
+  // one bulk copy of coil ci's spill tile into tiles[ci & 1] (thread 0)
   auto issue = [&](int ci) {
     const uint32_t b = smem_u32(&bar[ci & 1]);
     mbar_expect_tx(b, C::TILE_BYTES);
-    float2* dst = tiles + (ci & 1) * C::TILE_ELEMS;
-#pragma unroll
-    for (int bx = 0; bx < C::NBOX; ++bx)
-      tma_load_4d(smem_u32(dst + bx * C::BOX_KX * YT), &a.spill_map, y0, bx * C::BOX_KX, z, slot0 + ci, b);
+    bulk_copy_g2s(smem_u32(tiles + (ci & 1) * C::TILE_ELEMS),
+                  a.spill + spill_tile_offset(slot0 + ci, z, blockIdx.x, N0, N1, M2), C::TILE_BYTES, b);
   };
 
   float2 acc[LPT][E / 2];
@@ -871,7 +859,7 @@ inv_x_combine_kernel(const __grid_constant__ PassArgs a) {
       }
       float2 v[E];
 #pragma unroll
-      for (int r = 0; r < E; ++r) v[r] = tile[tile_pos<YT>(dout_index<M2>(t, r), line)];
+      for (int r = 0; r < E; ++r) v[r] = tile[spill_in_tile(dout_index<M2>(t, r), line, YT)];
       team_fft_dout_to_din<M2, 1, true>(v, t, buf, tw);
 #pragma unroll
       for (int e = 0; e < E / 2; ++e) {
