@@ -752,11 +752,13 @@ TEAM_SHAPE = {8: (4, 2), 16: (4, 4), 32: (8, 4), 64: (8, 8), 128: (16, 8), 256: 
 
 
 def column_kz(m0):
-    """kz held at each position p = t*E + r of a packed z column: the z transform's output
-    index (t + S*(r//S)) + E*(r%S) of lane t, register r (E, S: the team shape of m0)."""
+    """kz held at each position p of a packed z column: lane t's register r = 4j + c sits at
+    p = (j*S + t)*4 + c and holds the z transform's output index (t + S*(r//S)) + E*(r%S)
+    (E, S: the team shape of m0)."""
     E, S = TEAM_SHAPE[m0]
     p = np.arange(m0)
-    t, r = p // E, p % E
+    c, q = p % 4, p // 4
+    t, r = q % S, 4 * (q // S) + c
     return (t + S * (r // S)) + E * (r % S)
 
 

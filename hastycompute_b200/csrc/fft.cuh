@@ -417,12 +417,15 @@ __host__ __device__ inline void team_shape(int L, int* E, int* S) {
   }
 }
 
-// The frequency a z-column position p = t*E + r holds in the packed diagonal: the output
+// The frequency a z-column position p holds in the packed diagonal.  Lane t's registers
+// r = 4j + c (c < 4) sit at p = (j*S + t)*4 + c: the S lanes of a team read their j-th
+// group of four values as one contiguous run of S 16-byte vectors.  The value is the output
 // index dout_index<L>(t, r) = (t + S*(r/S)) + E*(r%S) of lane t, register r.
 __host__ __device__ inline int column_kz(int L, int p) {
   int E, S;
   team_shape(L, &E, &S);
-  const int t = p / E, r = p % E;
+  const int c = p % 4, q = p / 4;
+  const int t = q % S, r = 4 * (q / S) + c;
   return (t + S * (r / S)) + E * (r % S);
 }
 

@@ -331,15 +331,16 @@ expand_fwd_x_kernel(PassArgs a) {
   }
 }
 
-// Lane t's EZ diagonal values of one z column: the packed column stores them contiguously
-// at t*EZ (diag_pack_kernel), read as 16-byte vectors (EZ is a multiple of 4).
-template <int EZ>
+// Lane t's EZ diagonal values of one z column (team of SZ lanes): the packed column holds
+// registers 4j..4j+3 of lane t at (j*SZ + t)*4 (diag_pack_kernel), so the team's j-th
+// 16-byte loads cover SZ*16 contiguous bytes.
+template <int EZ, int SZ>
 __device__ __forceinline__ void load_tcol(float* dst, const float* col, int t) {
   static_assert(EZ % 4 == 0, "whole 16-byte vectors");
-  const float4* src = reinterpret_cast<const float4*>(col + t * EZ);
+  const float4* src = reinterpret_cast<const float4*>(col) + t;
 #pragma unroll
   for (int j = 0; j < EZ / 4; ++j) {
-    const float4 v = __ldg(src + j);
+    const float4 v = __ldg(src + j * SZ);
     dst[4 * j] = v.x;
     dst[4 * j + 1] = v.y;
     dst[4 * j + 2] = v.z;
@@ -473,7 +474,7 @@ plane_yz_kernel(PassArgs a) {
       float tnext[EZ];
       {
         const int col = team < H ? team : 0;
-        load_tcol<EZ>(tnext, T + (long long)(q * H + col) * M0, t);
+        load_tcol<EZ, SZ>(tnext, T + (long long)(q * H + col) * M0, t);
       }
   #pragma unroll 1
       for (int c0 = 0; c0 < H; c0 += C::NTEAMS_Z) {
@@ -485,7 +486,7 @@ plane_yz_kernel(PassArgs a) {
         for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
         if (c0 + C::NTEAMS_Z < H) {
           const int cn = c0 + C::NTEAMS_Z + team;
-          load_tcol<EZ>(tnext, T + (long long)(q * H + (cn < H ? cn : 0)) * M0, t);
+          load_tcol<EZ, SZ>(tnext, T + (long long)(q * H + (cn < H ? cn : 0)) * M0, t);
         }
         float2 v[EZ];
   #pragma unroll
@@ -696,7 +697,7 @@ plane_mod_kernel(PassArgs a) {
     if constexpr (kRegTw) load_lane_twiddles<M0>(twz, tw_z, t);
     auto tcol = [&](int col) { return T + (long long)((K / 2) * col + (q >> 1)) * M0; };
     float tnext[EZ];
-    load_tcol<EZ>(tnext, tcol(team < L ? team : 0), t);
+    load_tcol<EZ, SZ>(tnext, tcol(team < L ? team : 0), t);
 #pragma unroll 1
     for (int c0 = 0; c0 < L; c0 += C::NTEAMS_Z) {
       const int col = c0 + team;
@@ -707,7 +708,7 @@ plane_mod_kernel(PassArgs a) {
       for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
       if (c0 + C::NTEAMS_Z < L) {
         const int cn = c0 + C::NTEAMS_Z + team;
-        load_tcol<EZ>(tnext, tcol(cn < L ? cn : 0), t);
+        load_tcol<EZ, SZ>(tnext, tcol(cn < L ? cn : 0), t);
       }
       float2 v[EZ];
 #pragma unroll
@@ -829,6 +830,22 @@ inv_x_combine_kernel(PassArgs a) {
     for (int e = 0; e < E / 2; ++e) acc[l][e] = make_float2(0.f, 0.f);
 
   const float2* sm = a.sys_smaps[sys];
+  // coil ci's map values (or the multiplier) of this lane's x samples, fetched one coil
+  // ahead so their latency hides behind a whole coil's transform
+  auto load_maps = [&](int ci, float2 (&m)[LPT][E / 2]) {
+    const float2* ss = sm ? sm + ((long long)a.slot_coil[slot0 + ci] * N0 + z) * plane : nullptr;
+#pragma unroll
+    for (int l = 0; l < LPT; ++l) {
+      const long long row = (long long)(y0 + team + l * C::NTEAMS) * N2;
+#pragma unroll
+      for (int e = 0; e < E / 2; ++e) {
+        const int xi = din_index<M2>(t, e);
+        m[l][e] = ss ? ss[row + xi] : (a.mul ? a.mul[(long long)z * plane + row + xi] : make_float2(1.f, 0.f));
+      }
+    }
+  };
+  float2 mcur[LPT][E / 2];
+  if (ncoil > 0) load_maps(0, mcur);
   if (threadIdx.x == 0 && ncoil > 0) issue(0);
   int issued = ncoil > 0 ? 1 : 0;  // thread 0's count of copies issued
   int landed = 0;                  // copies whose wait completed
@@ -843,29 +860,27 @@ inv_x_combine_kernel(PassArgs a) {
     __syncthreads();
     if (abort_sh) break;  // read after the barrier: the same decision in every thread
     landed = ci + 1;
-    const int coil = a.slot_coil[slot0 + ci];
-    const float2* ss = sm ? sm + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
+    float2 mnext[LPT][E / 2];
+    if (ci + 1 < ncoil) load_maps(ci + 1, mnext);
     const float2* tile = tiles + (ci & 1) * C::TILE_ELEMS;
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
       const int line = team + l * C::NTEAMS;
-      const long long row = (long long)(y0 + line) * N2;
-      // coil-map (or multiplier) values first: their latency hides behind the FFT
-      float2 m[E / 2];
-#pragma unroll
-      for (int e = 0; e < E / 2; ++e) {
-        const int xi = din_index<M2>(t, e);
-        m[e] = ss ? ss[row + xi] : (a.mul ? a.mul[(long long)z * plane + row + xi] : make_float2(1.f, 0.f));
-      }
       float2 v[E];
 #pragma unroll
       for (int r = 0; r < E; ++r) v[r] = tile[spill_in_tile(dout_index<M2>(t, r), line, YT)];
       team_fft_dout_to_din<M2, 1, true>(v, t, buf, tw);
 #pragma unroll
       for (int e = 0; e < E / 2; ++e) {
-        const float2 val = ss ? cmulc(v[e], m[e]) : cmul(v[e], m[e]);
+        const float2 val = sm ? cmulc(v[e], mcur[l][e]) : cmul(v[e], mcur[l][e]);
         acc[l][e] = cadd(acc[l][e], val);
       }
+    }
+    if (ci + 1 < ncoil) {
+#pragma unroll
+      for (int l = 0; l < LPT; ++l)
+#pragma unroll
+        for (int e = 0; e < E / 2; ++e) mcur[l][e] = mnext[l][e];
     }
     __syncthreads();  // this tile buffer is refilled two coils later
   }
