@@ -429,6 +429,33 @@ __host__ __device__ inline int column_kz(int L, int p) {
   return (t + S * (r / S)) + E * (r % S);
 }
 
+// team_fft_dout_to_din with an unpadded exchange buffer of exactly L = E*S entries: entry
+// (row, col) of the E x S exchange lies at row*S + (col ^ (row % S)).  Both transpose
+// directions then touch S distinct banks per team, so a team can exchange inside any L
+// contiguous entries, e.g. the part of a tile it has just read into registers.
+template <int L, int DIR>
+__device__ __forceinline__ void team_fft_dout_to_din_xor(float2* v, int t, float2* buf, const float2* tw) {
+  constexpr int E = TeamCfg<L>::E, S = TeamCfg<L>::S;
+#pragma unroll
+  for (int c = 0; c < E / S; ++c) {
+    float2 u[S];
+#pragma unroll
+    for (int k2 = 0; k2 < S; ++k2) u[k2] = v[c * S + k2];
+    Dft<S, DIR>::run(u);
+#pragma unroll
+    for (int j = 0; j < S; ++j) buf[(t + S * c) * S + (j ^ t)] = u[j];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < E; ++k1) {
+    float2 w = tw[k1 * S + t];
+    if (DIR > 0) w.y = -w.y;
+    v[k1] = cmul(buf[k1 * S + (t ^ (k1 % S))], w);
+  }
+  __syncwarp();
+  Dft<E, DIR>::run(v);
+}
+
 // Index helpers for the two layouts.
 template <int L>
 HB_DEV int din_index(int t, int e) { return t + TeamCfg<L>::S * e; }

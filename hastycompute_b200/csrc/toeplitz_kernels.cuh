@@ -89,7 +89,10 @@ struct XPassCfg {
   // + two coil-map stages; pass C = two tiles + the exchange buffers; each + the M2-entry
   // twiddle table
   static constexpr int SMEM_F2 = TILE + 2 * SMT + M2;
-  static constexpr int SMEM_F2_C = 2 * TILE_ELEMS + NTEAMS * TBUF + M2;
+  // pass C: a team of S = 16 lanes with one line (LPT = 1) exchanges inside its share of
+  // the tile it has just read (no separate exchange buffers)
+  static constexpr bool C_IN_TILE = S == 16 && LPT == 1 && NTEAMS * M2 == TILE_ELEMS;
+  static constexpr int SMEM_F2_C = 2 * TILE_ELEMS + (C_IN_TILE ? 0 : NTEAMS * TBUF) + M2;
   static_assert(THREADS % 32 == 0, "x-pass CTA must be whole warps");
   static_assert((YT & (YT - 1)) == 0, "the tile swizzle needs a power-of-two tile height");
   static_assert(TILE_BYTES % 16 == 0 && (SMT * 8) % 16 == 0, "bulk copies move whole 16-byte units");
@@ -783,14 +786,14 @@ plane_mod_kernel(PassArgs a) {
 
 // ------------------------------------------------------------------------ pass C ----
 template <int N2, int YT>
-__global__ void __launch_bounds__(XPassCfg<N2, YT>::THREADS)
+__global__ void __launch_bounds__(XPassCfg<N2, YT>::THREADS, XPassCfg<N2, YT>::C_IN_TILE ? 3 : 1)
 inv_x_combine_kernel(PassArgs a) {
   using C = XPassCfg<N2, YT>;
   constexpr int M2 = C::M2, E = C::E, S = C::S, LPT = C::LPT;
   extern __shared__ __align__(128) float2 smem[];
   float2* tiles = smem;                          // 2 x spill tile [M2][YT] (swizzled)
-  float2* xbuf = tiles + 2 * C::TILE_ELEMS;      // teams' exchange buffers
-  float2* tw = xbuf + C::NTEAMS * C::TBUF;
+  float2* xbuf = tiles + 2 * C::TILE_ELEMS;      // teams' exchange buffers (unless in the tile)
+  float2* tw = xbuf + (C::C_IN_TILE ? 0 : C::NTEAMS * C::TBUF);
   __shared__ double red[32];
   __shared__ __align__(8) uint64_t bar[2];       // tile ci landed: bar[ci & 1], phase ci >> 1
   __shared__ int abort_sh;
@@ -830,22 +833,6 @@ inv_x_combine_kernel(PassArgs a) {
     for (int e = 0; e < E / 2; ++e) acc[l][e] = make_float2(0.f, 0.f);
 
   const float2* sm = a.sys_smaps[sys];
-  // coil ci's map values (or the multiplier) of this lane's x samples, fetched one coil
-  // ahead so their latency hides behind a whole coil's transform
-  auto load_maps = [&](int ci, float2 (&m)[LPT][E / 2]) {
-    const float2* ss = sm ? sm + ((long long)a.slot_coil[slot0 + ci] * N0 + z) * plane : nullptr;
-#pragma unroll
-    for (int l = 0; l < LPT; ++l) {
-      const long long row = (long long)(y0 + team + l * C::NTEAMS) * N2;
-#pragma unroll
-      for (int e = 0; e < E / 2; ++e) {
-        const int xi = din_index<M2>(t, e);
-        m[l][e] = ss ? ss[row + xi] : (a.mul ? a.mul[(long long)z * plane + row + xi] : make_float2(1.f, 0.f));
-      }
-    }
-  };
-  float2 mcur[LPT][E / 2];
-  if (ncoil > 0) load_maps(0, mcur);
   if (threadIdx.x == 0 && ncoil > 0) issue(0);
   int issued = ncoil > 0 ? 1 : 0;  // thread 0's count of copies issued
   int landed = 0;                  // copies whose wait completed
@@ -860,27 +847,35 @@ inv_x_combine_kernel(PassArgs a) {
     __syncthreads();
     if (abort_sh) break;  // read after the barrier: the same decision in every thread
     landed = ci + 1;
-    float2 mnext[LPT][E / 2];
-    if (ci + 1 < ncoil) load_maps(ci + 1, mnext);
-    const float2* tile = tiles + (ci & 1) * C::TILE_ELEMS;
+    const int coil = a.slot_coil[slot0 + ci];
+    const float2* ss = sm ? sm + (long long)coil * N0 * plane + (long long)z * plane : nullptr;
+    float2* tile = tiles + (ci & 1) * C::TILE_ELEMS;
 #pragma unroll
     for (int l = 0; l < LPT; ++l) {
       const int line = team + l * C::NTEAMS;
+      const long long row = (long long)(y0 + line) * N2;
+      // coil-map (or multiplier) values first: their latency hides behind the FFT
+      float2 m[E / 2];
+#pragma unroll
+      for (int e = 0; e < E / 2; ++e) {
+        const int xi = din_index<M2>(t, e);
+        m[e] = ss ? ss[row + xi] : (a.mul ? a.mul[(long long)z * plane + row + xi] : make_float2(1.f, 0.f));
+      }
       float2 v[E];
 #pragma unroll
       for (int r = 0; r < E; ++r) v[r] = tile[spill_in_tile(dout_index<M2>(t, r), line, YT)];
-      team_fft_dout_to_din<M2, 1, true>(v, t, buf, tw);
+      if constexpr (C::C_IN_TILE) {
+        __syncthreads();  // every team has its values: the tile becomes the exchange space
+        team_fft_dout_to_din_xor<M2, 1>(v, t, tile + team * M2, tw);
+        fence_proxy_async_smem();  // these writes precede the bulk copy that refills the tile
+      } else {
+        team_fft_dout_to_din<M2, 1, true>(v, t, buf, tw);
+      }
 #pragma unroll
       for (int e = 0; e < E / 2; ++e) {
-        const float2 val = sm ? cmulc(v[e], mcur[l][e]) : cmul(v[e], mcur[l][e]);
+        const float2 val = ss ? cmulc(v[e], m[e]) : cmul(v[e], m[e]);
         acc[l][e] = cadd(acc[l][e], val);
       }
-    }
-    if (ci + 1 < ncoil) {
-#pragma unroll
-      for (int l = 0; l < LPT; ++l)
-#pragma unroll
-        for (int e = 0; e < E / 2; ++e) mcur[l][e] = mnext[l][e];
     }
     __syncthreads();  // this tile buffer is refilled two coils later
   }
