@@ -29,12 +29,16 @@ namespace hb {
 
 // ------------------------------------------------------------------- spill layout ----
 // The spill holds, per (system, coil) slot, the image after the forward x transform:
-// [slot][z][yt][kx][yy'] with yt = y / YT, yy' = (y % YT) ^ (kx % YT), YT = spill_yt(N1).
+// [slot][z][yt][kx][yy'] with yt = y / YT, yy' = pos(y % YT) ^ (kx % YT), YT = spill_yt(N1),
+// pos(u) = 2 * (u % (YT/2)) + u / (YT/2).
 // * The (slot, z, yt) tile that passes A and C move is one contiguous M2 x YT block, so it
 //   travels as one bulk copy and lies in shared memory exactly as in global memory.
 // * The XOR puts the YT values of one kx row in an order that depends on kx, so a tile
 //   column (one y, consecutive kx: what one FFT team writes or reads) falls on distinct
 //   shared-memory banks without padding.
+// * pos interleaves the two halves of a kx row: y and y + YT/2 sit side by side (in either
+//   order after the XOR) in one aligned 16-byte pair, which is what a lane of an
+//   (YT/2)-lane FFT team of pass B needs for two of its registers.
 // * Row z of the (slot, kx) plane that pass B transforms is N1 / YT chunks of YT values
 //   (128 bytes for YT = 16), M2 * YT apart, rows M2 * N1 apart.
 __host__ __device__ constexpr int spill_yt(int N1) { return N1 < 16 ? N1 : 16; }
@@ -42,7 +46,12 @@ __host__ __device__ inline long long spill_tile_offset(int slot, int z, int yt, 
   const int YT = spill_yt(N1);
   return (((long long)slot * N0 + z) * (N1 / YT) + yt) * (long long)(M2 * YT);
 }
-__host__ __device__ constexpr int spill_in_tile(int kx, int yy, int YT) { return kx * YT + (yy ^ (kx & (YT - 1))); }
+__host__ __device__ constexpr int spill_pos(int yy, int YT) {
+  return YT < 2 ? yy : 2 * (yy % (YT / 2)) + yy / (YT / 2);
+}
+__host__ __device__ constexpr int spill_in_tile(int kx, int yy, int YT) {
+  return kx * YT + (spill_pos(yy, YT) ^ (kx & (YT - 1)));
+}
 __host__ __device__ inline long long spill_index(int slot, int z, int kx, int y, int N0, int N1, int M2) {
   const int YT = spill_yt(N1);
   return spill_tile_offset(slot, z, y / YT, N0, N1, M2) + spill_in_tile(kx, y % YT, YT);
@@ -63,9 +72,18 @@ struct SpillPlane {
     sw = kx & (YT - 1);
   }
   __device__ __forceinline__ long long off(int z, int y) const {
-    return z * rs + (long long)(y / YT) * cs + ((y % YT) ^ sw);
+    return z * rs + (long long)(y / YT) * cs + (spill_pos(y % YT, YT) ^ sw);
   }
   __device__ __forceinline__ float2& at(int z, int y) const { return base[off(z, y)]; }
+  // lo = at(z, y), hi = at(z, y + YT/2) for y % YT < YT/2, as one 16-byte load (YT >= 4;
+  // base is 16-byte aligned: kx * YT elements past a tile start)
+  __device__ __forceinline__ void pair(int z, int y, float2& lo, float2& hi) const {
+    const float4 w = *reinterpret_cast<const float4*>(
+        base + z * rs + (long long)(y / YT) * cs + ((2 * (y % (YT / 2))) ^ (sw & ~1)));
+    const bool swap = sw & 1;  // the XOR's low bit exchanges the two
+    lo = swap ? make_float2(w.z, w.w) : make_float2(w.x, w.y);
+    hi = swap ? make_float2(w.x, w.y) : make_float2(w.z, w.w);
+  }
 };
 
 // ---------------------------------------------------------------- launch geometry ----
@@ -656,13 +674,23 @@ plane_mod_kernel(PassArgs a) {
 #pragma unroll
     for (int e = 0; e < ER; ++e) cw[e] = circ[(din_index<L>(t, e) * q) % M1];
     float2 nv[NM][ER];  // the next row's values, loaded while the current one is transformed
-    {
-      const int z0 = tr < N0 ? tr : 0;
+    // With YT = 2*SR, y = t + SR*e and y + SR (registers e, e + 1 for even e) are one
+    // aligned 16-byte pair of the spill row: a team of SR lanes reads 16*SR contiguous bytes.
+    constexpr int YT = SpillPlane<N1>::YT;
+    constexpr bool kPair = YT == 2 * SR && L % YT == 0 && ER % 2 == 0;
+    auto load_row = [&](int zz) {
 #pragma unroll
-      for (int m = 0; m < NM; ++m)
+      for (int m = 0; m < NM; ++m) {
+        if constexpr (kPair) {
 #pragma unroll
-        for (int e = 0; e < ER; ++e) nv[m][e] = g.at(z0, din_index<L>(t, e) + L * m);
-    }
+          for (int e = 0; e < ER; e += 2) g.pair(zz, din_index<L>(t, e) + L * m, nv[m][e], nv[m][e + 1]);
+        } else {
+#pragma unroll
+          for (int e = 0; e < ER; ++e) nv[m][e] = g.at(zz, din_index<L>(t, e) + L * m);
+        }
+      }
+    };
+    load_row(tr < N0 ? tr : 0);
 #pragma unroll 1
     for (int it = 0; it < C::LPT; ++it) {
       const int z = tr + it * C::NTEAMS_R;
@@ -674,13 +702,7 @@ plane_mod_kernel(PassArgs a) {
         for (int m = 1; m < NM; ++m) acc = cadd(acc, rootK<K, -1>(nv[m][e], m * q));
         v[e] = q == 0 ? acc : cmul(acc, cw[e]);
       }
-      if (it + 1 < C::LPT) {
-        const int zn = z + C::NTEAMS_R < N0 ? z + C::NTEAMS_R : 0;
-#pragma unroll
-        for (int m = 0; m < NM; ++m)
-#pragma unroll
-          for (int e = 0; e < ER; ++e) nv[m][e] = g.at(zn, din_index<L>(t, e) + L * m);
-      }
+      if (it + 1 < C::LPT) load_row(z + C::NTEAMS_R < N0 ? z + C::NTEAMS_R : 0);
       team_fft_din_to_dout_r<L, -1, false>(v, t, buf, twr);
       if (z < N0) {
 #pragma unroll
