@@ -598,6 +598,19 @@ struct PlaneModCfg {
   static_assert(THREADS % SR == 0 && THREADS % SZ == 0, "teams must tile the CTA");
 };
 
+template <int V>
+struct IntC {
+  static constexpr int value = V;
+};
+// f(IntC<r>{}) for the run-time r in [0, K): one instantiation of f per value
+template <int K, int I = 0, class F>
+__device__ __forceinline__ void with_rank(int r, F&& f) {
+  if constexpr (I < K) {
+    if (r == I) f(IntC<I>{});
+    else with_rank<K, I + 1>(r, f);
+  }
+}
+
 // v * exp(DIR * 2*pi*i * p / K) for a runtime p (K = 4 or 8): rotations and one
 // multiply by sqrt(1/2) at most
 template <int K, int DIR>
@@ -664,7 +677,10 @@ plane_mod_kernel(PassArgs a) {
   // the K-th roots of unity, twiddles once by w_M1^(y'*q), then an L-point FFT.  Lane t
   // uses the same row-FFT twiddles (tw_r[k1*SR + t]) and fold twiddles w_M1^(y'*q) for
   // every row: they are read from shared memory once, into registers (stage 3 likewise).
-  {
+  // The rank is a compile-time constant inside (one copy of the stage per rank), so the
+  // fold's roots of unity and the rank-0 case cost no run-time selects.
+  with_rank<K>(q, [&](auto rank) {
+    constexpr int q = decltype(rank)::value;
     const int team = threadIdx.x / SR, t = threadIdx.x % SR;
     const int tr = row_of_team<SR, C::NTEAMS_R, N0>(team);
     float2* buf = xbuf + team * C::TBUF_R;
@@ -709,7 +725,7 @@ plane_mod_kernel(PassArgs a) {
         for (int r = 0; r < ER; ++r) P[z * LDP + dout_index<L>(t, r)] = v[r];
       }
     }
-  }
+  });
   __syncthreads();
 
   // stage 2: the CTA's L columns, M0-point FFT along z (upper half zero), x T,
