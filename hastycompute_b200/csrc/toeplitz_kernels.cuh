@@ -71,15 +71,17 @@ struct SpillPlane {
     cs = (long long)M2 * YT;
     sw = kx & (YT - 1);
   }
-  __device__ __forceinline__ long long off(int z, int y) const {
-    return z * rs + (long long)(y / YT) * cs + (spill_pos(y % YT, YT) ^ sw);
+  // Offsets within one plane fit in 32 bits: N0 * M2 * N1 <= 160 * 320 * 160 elements for
+  // every supported size (32-bit index arithmetic is the cheaper form).
+  __device__ __forceinline__ int off(int z, int y) const {
+    return z * (int)rs + (y / YT) * (int)cs + (spill_pos(y % YT, YT) ^ sw);
   }
   __device__ __forceinline__ float2& at(int z, int y) const { return base[off(z, y)]; }
   // lo = at(z, y), hi = at(z, y + YT/2) for y % YT < YT/2, as one 16-byte load (YT >= 4;
   // base is 16-byte aligned: kx * YT elements past a tile start)
   __device__ __forceinline__ void pair(int z, int y, float2& lo, float2& hi) const {
     const float4 w = *reinterpret_cast<const float4*>(
-        base + z * rs + (long long)(y / YT) * cs + ((2 * (y % (YT / 2))) ^ (sw & ~1)));
+        base + (z * (int)rs + (y / YT) * (int)cs + ((2 * (y % (YT / 2))) ^ (sw & ~1))));
     const bool swap = sw & 1;  // the XOR's low bit exchanges the two
     lo = swap ? make_float2(w.z, w.w) : make_float2(w.x, w.y);
     hi = swap ? make_float2(w.x, w.y) : make_float2(w.z, w.w);
@@ -739,17 +741,19 @@ plane_mod_kernel(PassArgs a) {
     auto tcol = [&](int col) { return T + (long long)((K / 2) * col + (q >> 1)) * M0; };
     float tnext[EZ];
     load_tcol<EZ, SZ>(tnext, tcol(team < L ? team : 0), t);
-#pragma unroll 1
+#pragma unroll
     for (int c0 = 0; c0 < L; c0 += C::NTEAMS_Z) {
       const int col = c0 + team;
-      const bool ok = col < L;
+      // team < NTEAMS_Z, so with L a multiple of NTEAMS_Z every column exists
+      constexpr bool kFull = L % C::NTEAMS_Z == 0;
+      const bool ok = kFull || col < L;
       const int colc = ok ? col : 0;
       float tv[EZ];
 #pragma unroll
       for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
       if (c0 + C::NTEAMS_Z < L) {
         const int cn = c0 + C::NTEAMS_Z + team;
-        load_tcol<EZ, SZ>(tnext, tcol(cn < L ? cn : 0), t);
+        load_tcol<EZ, SZ>(tnext, tcol(kFull || cn < L ? cn : 0), t);
       }
       float2 v[EZ];
 #pragma unroll
@@ -803,7 +807,10 @@ plane_mod_kernel(PassArgs a) {
     float2 cy[K];                   // w_M1^(y*qq), from registers
 #pragma unroll
     for (int qq = 1; qq < K; ++qq) cy[qq] = circ[(y * qq) % M1];
-    for (int i = threadIdx.x; i < ROWS * L; i += C::THREADS) {
+    static_assert((ROWS * L) % C::THREADS == 0, "stage-4 items per thread");
+#pragma unroll
+    for (int j = 0; j < ROWS * L / C::THREADS; ++j) {
+      const int i = threadIdx.x + j * C::THREADS;
       const int z = q * ROWS + i / L;
       float2 u[K];
       u[0] = R[0][z * LDP + y];
