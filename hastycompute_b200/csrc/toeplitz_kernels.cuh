@@ -709,7 +709,7 @@ plane_mod_kernel(PassArgs a) {
       }
     };
     load_row(tr < N0 ? tr : 0);
-#pragma unroll 1
+#pragma unroll 2
     for (int it = 0; it < C::LPT; ++it) {
       const int z = tr + it * C::NTEAMS_R;
       float2 v[ER];
@@ -779,7 +779,7 @@ plane_mod_kernel(PassArgs a) {
     float2* buf = xbuf + team * C::TBUF_R;
     float2 twr[ER];
     load_lane_twiddles<L>(twr, tw_r, t);
-#pragma unroll 1
+#pragma unroll 2
     for (int it = 0; it < C::LPT; ++it) {
       const int z = tr + it * C::NTEAMS_R;
       const int zc = z < N0 ? z : 0;
