@@ -267,7 +267,7 @@ int hb_plan_autotune(hb_plan* plan, int64_t nslots, void* workspace, size_t work
  *  - Sizes whose twiddle tables exceed the built-in table array return
  *    HB_ERR_UNSUPPORTED (every size hb_size_supported accepts fits).
  *  - Works on the calling thread's current device.  The first call on a device looks up
- *    the arrays' device addresses; make that first call before any stream capture.
+ *    the arrays' device addresses.
  *  - Every call copies its descriptor block (and, when the size differs from the
  *    previous call's on this device, the twiddle tables) from host memory with
  *    cudaMemcpyAsync on `stream` and then waits for `stream` with
