@@ -58,6 +58,7 @@ SIGNATURES = {
     "hb_plan_precision": (c_int, [c_void_p]),
     "hb_wait_status": (c_int, [c_int]),
     "hb_plan_inject_tc_stall": (c_int, [c_void_p, c_int]),
+    "hb_plan_inject_x_stall": (c_int, [c_void_p, c_int]),
     "hb_diag_packed_floats": (c_i64, [c_void_p]),
     "hb_diag_pack": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "hb_diag_build_workspace_bytes": (c_size, [c_void_p, c_i64]),

@@ -30,6 +30,7 @@ struct hb_plan {
   unsigned char* tc_ftab = nullptr;  // tensor-core pass A: DFT rows in operand layout
   int* tc_wait_error = nullptr;      // device address of g_tc_wait_error
   int tc_stall_chunk = -1;           // fault injection for tests (hb_plan_inject_tc_stall)
+  int x_stall_coil = -1;             // fault injection for tests (hb_plan_inject_x_stall)
 };
 
 namespace hb {
@@ -477,6 +478,7 @@ PassArgs group_pass_args(const hb_plan* p, const GroupWs& w, int64_t g, int64_t 
   a.accumulate = 0;
   a.dot_partials = nullptr;
   a.wait_error = p->tc_wait_error;
+  a.inject_stall = p->x_stall_coil + 1;
   return a;
 }
 
@@ -977,6 +979,13 @@ int hb_plan_inject_tc_stall(hb_plan* p, int chunk) {
   if (chunk < -1 || chunk >= p->N2 / tc::kKc)
     return fail(HB_ERR_INVALID, "hb_plan_inject_tc_stall: chunk must be -1 or in [0, nx / 16)");
   p->tc_stall_chunk = chunk;
+  return HB_OK;
+}
+
+int hb_plan_inject_x_stall(hb_plan* p, int coil) {
+  if (int r = check_plan(p)) return r;
+  if (coil < -1) return fail(HB_ERR_INVALID, "hb_plan_inject_x_stall: coil must be -1 or >= 0");
+  p->x_stall_coil = coil;
   return HB_OK;
 }
 

@@ -210,6 +210,8 @@ struct PassArgs {
   int accumulate;                  // 1: out += result, 0: out = result
   double* dot_partials;            // [nsys][nblocks_c] Re<x, out> partials (nullable)
   int prefetch_ahead;              // mod-4 plane pass: L2-prefetch distance in clusters (0 = off)
+  int inject_stall;                // tests only: pass C omits the tile copy of coil index
+                                   // inject_stall - 1 of every system (0 = off)
 };
 
 
@@ -865,6 +867,7 @@ inv_x_combine_kernel(PassArgs a) {
   const int slot0 = a.sys_slot0[sys], ncoil = a.sys_nslot[sys];
   // one bulk copy of coil ci's spill tile into tiles[ci & 1] (thread 0)
   auto issue = [&](int ci) {
+    if (a.inject_stall == ci + 1) return;  // a wait that nothing completes (fault injection)
     const uint32_t b = smem_u32(&bar[ci & 1]);
     mbar_expect_tx(b, C::TILE_BYTES);
     bulk_copy_g2s(smem_u32(tiles + (ci & 1) * C::TILE_ELEMS),

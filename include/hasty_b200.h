@@ -99,6 +99,12 @@ int hb_wait_status(int device);
  * the CTA returns without writing its output; the device stays usable and hb_wait_status
  * (or the CG's own check) reports it.  chunk = -1 turns it off (the default). */
 int hb_plan_inject_tc_stall(hb_plan* plan, int chunk);
+/* The same for the FP32 x passes: later inverse x passes (pass C) of this plan omit the
+ * bulk copy of the spill tile of coil index `coil` (0-based within each system), so each
+ * CTA's wait for it runs out after about one second and the CTA returns without writing
+ * its output; reported as above.  coil = -1 turns it off (the default).  Systems with
+ * fewer coils are not affected. */
+int hb_plan_inject_x_stall(hb_plan* plan, int coil);
 
 /* Number of floats of one packed diagonal (= 8 * nz * ny * nx).  Every packed diagonal
  * passed to the calls below must start on a 16-byte boundary (HB_ERR_INVALID otherwise):

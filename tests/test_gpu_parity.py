@@ -419,3 +419,35 @@ def test_bench_unpacks_the_packed_diagonal(cuda):
     got = bench.unpack_diagonal(plan, packed)(0)
     want = torch.from_numpy(T.real.astype(np.float32).astype(np.float64)).to(cuda)
     assert torch.allclose(got.real, want, rtol=1e-6, atol=0) and float(got.imag.abs().max()) == 0.0
+
+
+def test_x_pass_wait_that_runs_out_is_reported(cuda):
+    """Pass C made to wait for a spill tile that is never copied (hb_plan_inject_x_stall:
+    a wait that nothing completes): each CTA gives up after about a second and returns
+    without its output, the flag reaches the host through hb_wait_status and through the
+    CG's own check, and later calls on the same device are correct."""
+    shape = (8, 32, 32)  # 16 pass-C CTAs, all resident at once: about two seconds per launch
+    rng = np.random.default_rng(61)
+    T = O.toeplitz_diagonal(rng.uniform(-np.pi, np.pi, (3, 200)), shape)
+    sm = synth.coil_maps(2, shape, seed=62)
+    x = synth.gaussian_image(shape, seed=63)
+    plan = ToeplitzPlan(shape, cuda)
+    lib = plan.lib
+    packed = plan.pack_diagonal(_c64(T, cuda))
+    smt, xt = _c64(sm, cuda), _c64(x, cuda)
+    assert lib.hb_plan_inject_x_stall(plan._h, -2) == capi.HB_ERR_INVALID
+    capi.check(lib.hb_plan_inject_x_stall(plan._h, 1))
+    out = torch.empty_like(xt)
+    plan.sense_normal(xt, out, smt, packed)
+    with pytest.raises(capi.HastyError) as e:
+        plan.wait_status()
+    assert e.value.code == capi.HB_ERR_CUDA and "gave up waiting" in str(e.value)
+    plan.wait_status()  # read once, then cleared
+    b = _c64(O.sense_normal_toeplitz(x, sm, T), cuda)
+    with pytest.raises(capi.HastyError) as e:
+        plan.cg(torch.zeros_like(b), b, smt, packed, iters=1)
+    assert "gave up waiting" in str(e.value)
+    capi.check(lib.hb_plan_inject_x_stall(plan._h, -1))
+    plan.sense_normal(xt, out, smt, packed)
+    plan.wait_status()
+    assert O.rel_l2(_np(out), O.sense_normal_toeplitz(x, sm, T)) < TOL
