@@ -753,10 +753,6 @@ plane_mod_kernel(PassArgs a) {
       float tv[EZ];
 #pragma unroll
       for (int r = 0; r < EZ; ++r) tv[r] = tnext[r];
-      if (c0 + C::NTEAMS_Z < L) {
-        const int cn = c0 + C::NTEAMS_Z + team;
-        load_tcol<EZ, SZ>(tnext, tcol(kFull || cn < L ? cn : 0), t);
-      }
       float2 v[EZ];
 #pragma unroll
       for (int e = 0; e < EZ / 2; ++e) v[e] = P[din_index<M0>(t, e) * LDP + colc];
@@ -764,6 +760,10 @@ plane_mod_kernel(PassArgs a) {
       else team_fft_din_to_dout<M0, -1, true>(v, t, buf, tw_z);
 #pragma unroll
       for (int r = 0; r < EZ; ++r) v[r] = cscale(v[r], tv[r]);
+      if (c0 + C::NTEAMS_Z < L) {
+        const int cn = c0 + C::NTEAMS_Z + team;
+        load_tcol<EZ, SZ>(tnext, tcol(kFull || cn < L ? cn : 0), t);
+      }
       if constexpr (kRegTw) team_fft_dout_to_din_r<M0, 1, true>(v, t, buf, twz);
       else team_fft_dout_to_din<M0, 1, true>(v, t, buf, tw_z);
       if (ok) {
